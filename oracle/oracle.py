@@ -1,0 +1,162 @@
+"""ctypes wrapper of the CPU oracle (liboracle.so) — TEST INFRASTRUCTURE ONLY.
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` use
+this module, and only as the checker / the timed CPU baseline. The shipped library never
+imports it.
+
+``OracleState`` restates the reference's host driver: ``step!`` (driver.jl:20-37),
+``evolve!`` (driver.jl:48-71), ``compute_dt`` (timestep.jl:37-46) and the diagnostics
+(diagnostics.jl:6-55, ct.jl:176-201), with the scalar arithmetic done in the state's
+precision T exactly where the reference does it in T.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+RECON = {"plm": 0, "ppm": 1, "plm_minmod": 2}
+RIEMANN = {"hlld": 0, "hll": 1, "llf": 2}
+BC = {"periodic": 0, "outflow": 1, "reflecting": 2}
+GLM_CR = 0.18
+N_WORK = 15
+
+
+class OracleParams(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("bc", ctypes.c_int * 3), ("recon", ctypes.c_int), ("riemann", ctypes.c_int),
+                ("gamma", ctypes.c_double), ("smallr", ctypes.c_double), ("pfl", ctypes.c_double),
+                ("llf_dmin", ctypes.c_double), ("llf_pmin", ctypes.c_double)]
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        _LIB = ctypes.CDLL(path)
+        P = ctypes.POINTER(OracleParams)
+        vp = ctypes.c_void_p
+        d = ctypes.c_double
+        for suf in ("f32", "f64"):
+            getattr(_LIB, f"oracle_step_glm_{suf}").argtypes = [P, vp, vp, d, d, d, vp]
+            getattr(_LIB, f"oracle_step_ct_{suf}").argtypes = [P, vp, vp, vp, vp, d, vp, vp]
+            for name in ("max_wavespeed",):
+                f = getattr(_LIB, f"oracle_{name}_{suf}")
+                f.argtypes = [P, vp]
+                f.restype = d
+            for name in ("max_divb", "max_divb_face"):
+                f = getattr(_LIB, f"oracle_{name}_{suf}")
+                f.argtypes = [P, vp, d]
+                f.restype = d
+            getattr(_LIB, f"oracle_ct_faces_from_potential_{suf}").argtypes = [P, vp, vp, vp, d]
+            getattr(_LIB, f"oracle_totals_{suf}").argtypes = [P, vp, vp]
+    return _LIB
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class OracleState:
+    """Host mirror of the reference ``MHDState`` driven by the oracle."""
+
+    def __init__(self, dims, dx, dtype=np.float32, gamma=5 / 3, smallr=1e-6, pfl=1e-7,
+                 llf_dmin=1e-4, llf_pmin=0.0, riemann="hlld", recon="plm", bcs=("periodic",) * 3,
+                 mhd_solver="glm", compensated=False):
+        self.dims = tuple(int(d) for d in dims)
+        self.nc = int(np.prod(self.dims))
+        self.T = np.dtype(dtype).type
+        self.dx = self.T(dx)
+        self.gamma = self.T(gamma)
+        self.mhd_solver = mhd_solver
+        if mhd_solver == "ct" and any(b != "periodic" for b in bcs):
+            raise ValueError("mhd_solver='ct' requires all-periodic boundaries")
+        self.p = OracleParams(self.dims[0], self.dims[1], self.dims[2], (ctypes.c_int * 3)(*[BC[b] for b in bcs]),
+                              RECON[recon], RIEMANN[riemann], float(self.gamma), float(self.T(smallr)),
+                              float(self.T(pfl)), float(self.T(llf_dmin)), float(self.T(llf_pmin)))
+        self.U = np.zeros((9, self.nc), dtype=dtype)
+        self.scratch = np.zeros_like(self.U)
+        self.faces = np.zeros((3, self.nc), dtype=dtype) if mhd_solver == "ct" else None
+        self.work = np.zeros((N_WORK, self.nc), dtype=dtype) if mhd_solver == "ct" else None
+        self.resid = np.zeros((7, self.nc), dtype=dtype) if compensated else None
+        self.face_resid = np.zeros((3, self.nc), dtype=dtype) if (compensated and mhd_solver == "ct") else None
+        self._suf = "f32" if self.T is np.float32 else "f64"
+
+    def _f(self, name):
+        return getattr(lib(), f"oracle_{name}_{self._suf}")
+
+    # -- the step (driver.jl:20-37, integrator_ref.jl:210-220, ct.jl:158-173) ----------------
+    def step(self, dt, ch=None, glm_cr=GLM_CR):
+        T = self.T
+        dtdx = T(T(dt) / self.dx)
+        if self.mhd_solver == "ct":
+            self._f("step_ct")(ctypes.byref(self.p), _ptr(self.U), _ptr(self.scratch), _ptr(self.faces),
+                               _ptr(self.work), float(dtdx), _ptr(self.resid), _ptr(self.face_resid))
+        else:
+            if ch is None:
+                raise ValueError("step needs the GLM cleaning speed ch")
+            decay = T(np.exp(T(-T(glm_cr) * T(ch) * T(dt) / self.dx)))
+            self._f("step_glm")(ctypes.byref(self.p), _ptr(self.U), _ptr(self.scratch), float(dtdx),
+                                float(T(ch)), float(decay), _ptr(self.resid))
+        self.U, self.scratch = self.scratch, self.U
+
+    def max_wavespeed(self):
+        return self.T(self._f("max_wavespeed")(ctypes.byref(self.p), _ptr(self.U)))
+
+    def compute_dt(self, cfl=0.4):
+        T = self.T
+        smax = self.max_wavespeed()
+        dt = T(T(cfl) * self.dx / max(smax, np.finfo(T).eps))
+        return dt, smax
+
+    def evolve(self, tfinal, cfl=0.4, glm_ch_fac=1.0, glm_cr=GLM_CR, callback=None):
+        T = self.T
+        t, n, tf = 0.0, 0, float(tfinal)
+        while t < tf * (1 - 1e-9):
+            dt, smax = self.compute_dt(cfl)
+            if self.mhd_solver == "ct":
+                ch = T(0)
+                dtf = float(dt)
+            else:
+                ch = T(T(glm_ch_fac) * smax)
+                dtf = float(dt) * float(smax) / float(max(smax, ch))
+            if t + dtf > tf:
+                dtf = tf - t
+            self.step(dtf, ch=ch, glm_cr=glm_cr)
+            t += dtf
+            n += 1
+            if callback is not None:
+                callback(self, t, n)
+        return t, n
+
+    # -- diagnostics ----------------------------------------------------------------------
+    def max_divb(self):
+        return self._f("max_divb")(ctypes.byref(self.p), _ptr(self.U), float(self.dx))
+
+    def max_divb_face(self):
+        return self._f("max_divb_face")(ctypes.byref(self.p), _ptr(self.faces), float(self.dx))
+
+    def conserved_totals(self):
+        out = np.zeros(8)
+        self._f("totals")(ctypes.byref(self.p), _ptr(self.U), _ptr(out))
+        dV = float(self.dx) ** 3
+        keys = ("mass", "momx", "momy", "momz", "energy", "Bx", "By", "Bz")
+        return {k: v * dV for k, v in zip(keys, out)}
+
+    def ct_faces_from_potential(self, A):
+        A = np.ascontiguousarray(np.asarray(A, dtype=self.U.dtype).reshape(3, self.nc))
+        self._f("ct_faces_from_potential")(ctypes.byref(self.p), _ptr(A), _ptr(self.faces), _ptr(self.U),
+                                           float(self.dx))
+        if self.face_resid is not None:
+            self.face_resid[:] = 0
