@@ -1,0 +1,173 @@
+/*
+ * pmfmhd.h — C ABI of libpmfmhd.so, a B200 (sm_100a) implementation of the PMFGLM
+ * ideal-MHD Godunov step (MUSCL-Hancock, MC-PLM / PPM / minmod reconstruction,
+ * HLLD / HLL / LLF Riemann solvers, Dedner GLM cleaning or face-staggered CT).
+ *
+ * Every field pointer is a DEVICE pointer to caller-owned FP32 storage in the
+ * reference's SoA layout: nine arrays U = (rho, rho*vx, rho*vy, rho*vz, E, Bx, By, Bz, psi)
+ * of nc = nx*ny*nz values each, cell (i,j,k) (0-based) at ((k*ny)+j)*nx+i (x fastest),
+ * exactly MHDKernels' `linidx` (lib/MHDKernels/src/state.jl:95). The library never frees
+ * caller memory; it allocates only small internal workspace owned by a pmfmhd_ctx.
+ *
+ * All calls return 0 on success or a negative PMFMHD_E* code (pmfmhd_strerror). Work is
+ * enqueued on the caller's stream (a cudaStream_t passed as void*; NULL = legacy default
+ * stream). Calls whose result is a host value synchronise that stream before returning.
+ */
+#ifndef PMFMHD_H
+#define PMFMHD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PMFMHD_OK 0
+#define PMFMHD_EINVAL (-1)        /* null pointer, unknown code, non-finite scalar */
+#define PMFMHD_ESHAPE (-2)        /* grid extent out of range */
+#define PMFMHD_ECUDA (-3)         /* CUDA runtime error (message: pmfmhd_last_cuda_error) */
+#define PMFMHD_ETIMEOUT (-4)      /* a bounded device-side wait gave up */
+#define PMFMHD_EINADMISSIBLE (-5) /* non-finite / non-positive state found by a check */
+#define PMFMHD_ENOMEM (-6)        /* workspace allocation failed */
+#define PMFMHD_EUNSUPPORTED (-7)  /* combination not provided (e.g. CT with non-periodic BCs) */
+
+/* Reconstruction codes (glm_physics.jl:202-207). */
+#define PMFMHD_RECON_PLM 0        /* MonCen (MC) PLM */
+#define PMFMHD_RECON_PPM 1        /* local CW84 PPM */
+#define PMFMHD_RECON_PLM_MINMOD 2 /* minmod PLM */
+/* Riemann solver codes (glm_physics.jl:309-314). */
+#define PMFMHD_RIEMANN_HLLD 0
+#define PMFMHD_RIEMANN_HLL 1
+#define PMFMHD_RIEMANN_LLF 2
+/* Boundary codes (boundary.jl:152-159). */
+#define PMFMHD_BC_PERIODIC 0
+#define PMFMHD_BC_OUTFLOW 1
+#define PMFMHD_BC_REFLECT 2
+
+/* Grid and run parameters: the scalar fields of MHDState (state.jl:63-79). */
+typedef struct pmfmhd_grid {
+  int32_t nx, ny, nz;
+  int32_t bc[3];   /* per axis, PMFMHD_BC_* */
+  int32_t recon;   /* PMFMHD_RECON_* */
+  int32_t riemann; /* PMFMHD_RIEMANN_* */
+  float dx, gamma, smallr, pfl, llf_dmin, llf_pmin;
+} pmfmhd_grid;
+
+/* Opaque per-device context: reduction workspace, tile autotuning table, cached graphs. */
+typedef struct pmfmhd_ctx pmfmhd_ctx;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int pmfmhd_version(void);
+const char* pmfmhd_strerror(int code);
+/* Text of the last CUDA error seen by this thread (empty if none). */
+const char* pmfmhd_last_cuda_error(void);
+
+/* Create / destroy a context on CUDA device `device` (the device is made current). */
+int pmfmhd_create(int device, pmfmhd_ctx** out);
+int pmfmhd_destroy(pmfmhd_ctx* ctx);
+
+/*
+ * One GLM Godunov step: read U, write Unew (distinct buffers), psi damped by `decay`.
+ * Replaces the KernelAbstractions launch `_cube_launch!(Val(:raw), CUDABackend, s, dt, ch, decay)`
+ * (lib/MHDKernels/ext/MHDKernelsCUDAExt.jl:22-26, integrator_cube.jl:467-476) and equally
+ * `step_ref!` (integrator_ref.jl:210-220): U = s.U, Unew = s.scratch; the caller swaps.
+ * dt is the step, ch the GLM cleaning speed, decay = exp(-cr*ch*dt/dx) (driver.jl:29).
+ * resid: NULL for the plain FP32 update, or 7 device arrays of Kahan remainders
+ * (rho*vx, rho*vy, rho*vz, E, Bx, By, Bz), zero-initialised by the caller and kept across
+ * steps (compensated update, glm_physics.jl:349-359, extended to momentum).
+ * The new state's max signal speed max(|v_d| + c_f,d) is reduced in the same launch and
+ * can be read with pmfmhd_last_wavespeed.
+ */
+int pmfmhd_step_glm(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],
+                    float dt, float ch, float decay, float* const resid[7], void* stream);
+
+/*
+ * One constrained-transport step (mhd_solver=:ct): Godunov stage with the staggered
+ * normal field on every face, Gardiner-Stone 2005 edge EMFs, face curl update and the
+ * face-averaged cell B. Replaces `step!`'s CT branch: `step_ref!(s, dt; ch=0, decay=1)`
+ * followed by `ct_update!` (driver.jl:22-27, integrator_ref.jl:210-220, ct.jl:158-173).
+ * ct_packed is the reference's CTState buffer (state.jl:44-58): 21*nc floats, slots
+ * bxf,byf,bzf | mfx,mfy,mfz | fxby,fxbz,fybx,fybz,fzbx,fzby | ecx,ecy,ecz | ex,ey,ez |
+ * rbx,rby,rbz. Slots 0-2 are updated in place, 3-17 are workspace, 18-20 hold the face
+ * Kahan remainders used when compensate_faces != 0. Requires all-periodic boundaries.
+ * resid: NULL or 7 remainder arrays as for pmfmhd_step_glm (the B slots are unused).
+ */
+int pmfmhd_step_ct(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],
+                   float* ct_packed, float dt, float* const resid[7], int compensate_faces, void* stream);
+
+/*
+ * Max signal speed max over cells and axes of |v_d| + c_fast,d (timestep.jl:4-14,
+ * `max_wavespeed!` :17-23). Blocking; *smax receives the host value.
+ */
+int pmfmhd_max_wavespeed(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], float* smax,
+                         void* stream);
+/* CFL step dt = cfl*dx/max(smax, eps) and smax (timestep.jl:37-41, `compute_dt!`). Blocking. */
+int pmfmhd_compute_dt(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], float cfl, float* dt,
+                      float* smax, void* stream);
+/* Max signal speed of the state written by the last pmfmhd_step_glm / pmfmhd_step_ct on
+ * this context (reduced on the device in that launch). Blocking. */
+int pmfmhd_last_wavespeed(pmfmhd_ctx* ctx, float* smax, void* stream);
+
+/* Max |div B| by BC-aware centred differences (diagnostics.jl:6-36). FP64 result. Blocking. */
+int pmfmhd_max_divb(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], double* out, void* stream);
+/* Max face divergence |sum_d (b_d[upper]-b_d[lower])|/dx of a CT face field (ct.jl:176-201). */
+int pmfmhd_max_divb_face(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* ct_packed, double* out,
+                         void* stream);
+/* FP64 volume integrals (mass, momx, momy, momz, energy, Bx, By, Bz) * dx^3
+ * (diagnostics.jl:44-55, `conserved_totals`). Blocking. */
+int pmfmhd_conserved_totals(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], double out[8],
+                            void* stream);
+
+/*
+ * CT initialisation from an EDGE-centred vector potential A (3 device arrays, Ax at
+ * (i,j-1/2,k-1/2), Ay at (i-1/2,j,k-1/2), Az at (i-1/2,j-1/2,k)): faces = discrete curl,
+ * cell B = face average, E adjusted to keep the thermal pressure, psi = 0, face remainders
+ * zeroed (ct.jl:310-345 `ct_faces_from_potential!`, :205-236).
+ */
+int pmfmhd_ct_faces_from_potential(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const A[3],
+                                   float* const U[9], float* ct_packed, void* stream);
+
+/*
+ * nsteps GLM steps with a fixed dt/ch/decay, ping-ponging between U and scratch, recorded
+ * once into a CUDA graph per (grid, buffers, nsteps) and replayed: the warm throughput
+ * loop of scripts/benchmark.jl:53-62 (`advance()` repeated). After an even number of
+ * steps the state is in U, after an odd number in scratch.
+ */
+int pmfmhd_run_glm(pmfmhd_ctx* ctx, const pmfmhd_grid* g, float* const U[9], float* const scratch[9],
+                   int nsteps, float dt, float ch, float decay, float* const resid[7], void* stream);
+
+/*
+ * Batched form: many independent periodic boxes of uneven sizes advanced together.
+ * Each box carries its own grid, buffers, solver and CFL settings; one pmfmhd_batch_step
+ * advances every box by one step with its own device-computed dt (CFL on the box's
+ * current state, ch = glm_ch_fac*smax, decay = exp(-glm_cr*ch*dt/dx), as `evolve!`,
+ * driver.jl:48-71), using one persistent work-queued launch per solver family. Steps
+ * are recorded into a CUDA graph on first use. No reference counterpart beyond
+ * looping `evolve!` over boxes.
+ */
+typedef struct pmfmhd_box {
+  pmfmhd_grid grid;
+  float* U[9];
+  float* scratch[9];
+  float* ct_packed; /* NULL for GLM boxes; 21*nc floats for CT boxes */
+  float* resid[7];  /* all NULL, or 7 remainder arrays (compensated update) */
+  int32_t mhd_solver; /* 0 = GLM, 1 = CT */
+  float cfl, glm_ch_fac, glm_cr;
+} pmfmhd_box;
+typedef struct pmfmhd_batch pmfmhd_batch;
+int pmfmhd_batch_create(pmfmhd_ctx* ctx, const pmfmhd_box* boxes, int nbox, pmfmhd_batch** out);
+int pmfmhd_batch_step(pmfmhd_batch* b, int nsteps, void* stream);
+/* Per-box results after the last step: time advanced, current-state index (0: U, 1: scratch),
+ * last dt. Any pointer may be NULL. Blocking. */
+int pmfmhd_batch_query(pmfmhd_batch* b, double* t, int32_t* parity, float* dt);
+int pmfmhd_batch_destroy(pmfmhd_batch* b);
+
+/* Tile autotuning: time the candidate tile shapes for this grid/solver on scratch copies
+ * of U and remember the fastest in the context (used by every later step). Blocking. */
+int pmfmhd_autotune(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], int mhd_solver,
+                    int compensated, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PMFMHD_H */

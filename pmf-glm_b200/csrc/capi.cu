@@ -1,0 +1,525 @@
+// C ABI of libpmfmhd.so: argument checks, tile selection, launches, CUDA-graph replay of
+// fixed-dt step sequences, and the FP64 diagnostics. See include/pmfmhd.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/pmfmhd.h"
+#include "aux_kernels.cuh"
+#include "dispatch.h"
+#include "step_kernel.cuh"
+
+using namespace pmf;
+
+namespace {
+
+thread_local std::string g_last_cuda;
+
+#define PMF_CK(call)                                                              \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess) {                                                      \
+      g_last_cuda = std::string(#call) + ": " + cudaGetErrorString(e_);            \
+      return PMFMHD_ECUDA;                                                        \
+    }                                                                             \
+  } while (0)
+
+constexpr int kTotBlocksMax = 1024;
+
+struct TuneKey {
+  int nx, ny, nz, ct, comp, recon, rsol;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(nx, ny, nz, ct, comp, recon, rsol) < std::tie(o.nx, o.ny, o.nz, o.ct, o.comp, o.recon, o.rsol);
+  }
+};
+struct Tune {
+  int ty, tz;
+};
+
+struct GraphEntry {
+  std::vector<unsigned char> key;
+  cudaGraphExec_t exec;
+};
+
+}  // namespace
+
+struct pmfmhd_ctx {
+  int device = 0;
+  int sms = 148;
+  unsigned int* d_smax = nullptr;           // bits of the last step's max signal speed
+  unsigned long long* d_u64 = nullptr;      // bits of an FP64 max
+  double* d_partial = nullptr;              // totals partials
+  double* d_tot = nullptr;                  // totals
+  unsigned char* h_pin = nullptr;           // pinned host landing area
+  cudaStream_t cap = nullptr;               // stream used to record graphs
+  std::map<TuneKey, Tune> tune;
+  std::vector<GraphEntry> graphs;
+  std::mutex mu;
+};
+
+namespace {
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int check_grid(const pmfmhd_grid* g) {
+  if (g == nullptr) return PMFMHD_EINVAL;
+  if (g->nx < 1 || g->ny < 1 || g->nz < 1) return PMFMHD_ESHAPE;
+  const long long nc = (long long)g->nx * g->ny * g->nz;
+  if (nc >= (1LL << 31)) return PMFMHD_ESHAPE;
+  for (int d = 0; d < 3; ++d)
+    if (g->bc[d] < 0 || g->bc[d] > 2) return PMFMHD_EINVAL;
+  if (g->recon < 0 || g->recon > 2 || g->riemann < 0 || g->riemann > 2) return PMFMHD_EINVAL;
+  if (!(g->dx > 0.0f) || !std::isfinite(g->dx) || !(g->gamma > 1.0f) || !std::isfinite(g->gamma))
+    return PMFMHD_EINVAL;
+  if (!std::isfinite(g->smallr) || !std::isfinite(g->pfl) || !std::isfinite(g->llf_dmin) ||
+      !std::isfinite(g->llf_pmin))
+    return PMFMHD_EINVAL;
+  return PMFMHD_OK;
+}
+bool all_periodic(const pmfmhd_grid* g) {
+  return g->bc[0] == BC_PERIODIC && g->bc[1] == BC_PERIODIC && g->bc[2] == BC_PERIODIC;
+}
+template <class P> bool nonnull(P* const* v, int n) {
+  if (v == nullptr) return false;
+  for (int i = 0; i < n; ++i)
+    if (v[i] == nullptr) return false;
+  return true;
+}
+// resid is either NULL / all-NULL (plain update) or 7 non-null pointers
+int resid_mode(float* const* r, bool* comp) {
+  *comp = false;
+  if (r == nullptr) return PMFMHD_OK;
+  int n = 0;
+  for (int i = 0; i < 7; ++i) n += r[i] != nullptr;
+  if (n == 0) return PMFMHD_OK;
+  if (n != 7) return PMFMHD_EINVAL;
+  *comp = true;
+  return PMFMHD_OK;
+}
+Phys phys_of(const pmfmhd_grid* g) { return Phys{g->gamma, g->smallr, g->pfl, g->llf_dmin, g->llf_pmin}; }
+long long ncells(const pmfmhd_grid* g) { return (long long)g->nx * g->ny * g->nz; }
+int aux_blocks(const pmfmhd_ctx* c, long long nc) {
+  long long b = (nc + AUX_THREADS - 1) / AUX_THREADS;
+  long long cap = (long long)c->sms * 8;
+  return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+}
+
+Tune default_tune(const pmfmhd_ctx* c, const pmfmhd_grid* g) {
+  Tune t;
+  t.ty = g->ny >= 8 ? 8 : 4;
+  const long long cols = (long long)((g->nx + TILE_X - 1) / TILE_X) * ((g->ny + t.ty - 1) / t.ty);
+  // enough CTAs for about two resident waves, but chunks of at least 16 planes
+  long long want = (2LL * c->sms + cols - 1) / cols;
+  int nzc = (int)std::max<long long>(1, std::min<long long>(want, (g->nz + 15) / 16));
+  t.tz = (g->nz + nzc - 1) / nzc;
+  return t;
+}
+
+Tune tune_for(pmfmhd_ctx* c, const pmfmhd_grid* g, bool ct, bool comp) {
+  std::lock_guard<std::mutex> lk(c->mu);
+  auto it = c->tune.find(TuneKey{g->nx, g->ny, g->nz, ct, comp, g->recon, g->riemann});
+  if (it != c->tune.end()) return it->second;
+  return default_tune(c, g);
+}
+
+int launch_step(const pmfmhd_grid* g, StepArgs& a, Tune t, bool ct, bool comp, cudaStream_t s) {
+  StepKernelInfo k = step_kernel_info(t.ty, g->recon, g->riemann, ct, comp);
+  if (k.fn == nullptr) return PMFMHD_EUNSUPPORTED;
+  PMF_CK(cudaFuncSetAttribute((const void*)k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_bytes));
+  a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
+  for (int d = 0; d < 3; ++d) a.bc[d] = g->bc[d];
+  a.ntx = (g->nx + TILE_X - 1) / TILE_X;
+  a.nty = (g->ny + t.ty - 1) / t.ty;
+  a.tz = t.tz;
+  a.nzc = (g->nz + t.tz - 1) / t.tz;
+  a.P = phys_of(g);
+  const long long blocks = (long long)a.ntx * a.nty * a.nzc;
+  if (blocks >= (1LL << 31)) return PMFMHD_ESHAPE;
+  void* args[] = {(void*)&a};
+  PMF_CK(cudaLaunchKernel((const void*)k.fn, dim3((unsigned)blocks), dim3(k.threads), args, k.smem_bytes, s));
+  return PMFMHD_OK;
+}
+
+void fill_glm_args(StepArgs& a, const float* const U[9], float* const Un[9], float* const resid[7], bool comp,
+                   float dtdx, float ch, float decay, unsigned int* smax_bits) {
+  std::memset(&a, 0, sizeof(a));
+  for (int f = 0; f < 9; ++f) { a.U[f] = U[f]; a.Un[f] = Un[f]; }
+  if (comp)
+    for (int i = 0; i < 7; ++i) a.resid[i] = resid[i];
+  a.dtdx = dtdx; a.ch = ch; a.decay = decay;
+  a.smax_bits = smax_bits;
+  a.dscal = nullptr;
+}
+
+int enqueue_glm(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Un[9], float dt,
+                float ch, float decay, float* const resid[7], bool comp, cudaStream_t s) {
+  StepArgs a;
+  const float dtdx = dt / g->dx;  // T(dt)/s.dx (integrator_ref.jl:211)
+  fill_glm_args(a, U, Un, resid, comp, dtdx, ch, decay, c->d_smax);
+  PMF_CK(cudaMemsetAsync(c->d_smax, 0, sizeof(unsigned int), s));
+  return launch_step(g, a, tune_for(c, g, false, comp), false, comp, s);
+}
+
+int enqueue_ct(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Un[9], float* ct, float dt,
+               float* const resid[7], bool comp, bool comp_faces, cudaStream_t s) {
+  const long long nc = ncells(g);
+  const float dtdx = dt / g->dx;
+  StepArgs a;
+  fill_glm_args(a, U, Un, resid, comp, dtdx, 0.0f, 1.0f, nullptr);
+  for (int d = 0; d < 3; ++d) a.face[d] = ct + (size_t)(CT_BXF + d) * nc;
+  for (int k = 0; k < CT_NWORK; ++k) a.work[k] = ct + (size_t)(CT_MFX + k) * nc;
+  int rc = launch_step(g, a, tune_for(c, g, true, comp), true, comp, s);
+  if (rc != PMFMHD_OK) return rc;
+  const int nb = aux_blocks(c, nc);
+  ct_emf_kernel<<<nb, AUX_THREADS, 0, s>>>(ct, g->nx, g->ny, g->nz);
+  if (comp_faces) ct_face_kernel<true><<<nb, AUX_THREADS, 0, s>>>(ct, g->nx, g->ny, g->nz, dtdx);
+  else ct_face_kernel<false><<<nb, AUX_THREADS, 0, s>>>(ct, g->nx, g->ny, g->nz, dtdx);
+  PMF_CK(cudaMemsetAsync(c->d_smax, 0, sizeof(unsigned int), s));
+  MPtr9 un;
+  for (int f = 0; f < 9; ++f) un.p[f] = Un[f];
+  ct_bcc_kernel<<<nb, AUX_THREADS, 0, s>>>(ct, un, g->nx, g->ny, g->nz, phys_of(g), c->d_smax);
+  PMF_CK(cudaGetLastError());
+  return PMFMHD_OK;
+}
+
+int read_smax(pmfmhd_ctx* c, float* out, cudaStream_t s) {
+  PMF_CK(cudaMemcpyAsync(c->h_pin, c->d_smax, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+  PMF_CK(cudaStreamSynchronize(s));
+  unsigned int bits;
+  std::memcpy(&bits, c->h_pin, sizeof(bits));
+  float v;
+  std::memcpy(&v, &bits, sizeof(v));
+  *out = v;
+  return PMFMHD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pmfmhd_version(void) { return 100; }
+
+const char* pmfmhd_strerror(int code) {
+  switch (code) {
+    case PMFMHD_OK: return "ok";
+    case PMFMHD_EINVAL: return "invalid argument";
+    case PMFMHD_ESHAPE: return "invalid grid shape";
+    case PMFMHD_ECUDA: return "CUDA error";
+    case PMFMHD_ETIMEOUT: return "device wait timed out";
+    case PMFMHD_EINADMISSIBLE: return "inadmissible state";
+    case PMFMHD_ENOMEM: return "out of memory";
+    case PMFMHD_EUNSUPPORTED: return "unsupported combination";
+  }
+  return "unknown error";
+}
+
+const char* pmfmhd_last_cuda_error(void) { return g_last_cuda.c_str(); }
+
+int pmfmhd_create(int device, pmfmhd_ctx** out) {
+  if (out == nullptr) return PMFMHD_EINVAL;
+  *out = nullptr;
+  PMF_CK(cudaSetDevice(device));
+  pmfmhd_ctx* c = new pmfmhd_ctx();
+  c->device = device;
+  if (cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) c->sms = 148;
+  if (cudaMalloc(&c->d_smax, 256) != cudaSuccess || cudaMalloc(&c->d_u64, 256) != cudaSuccess ||
+      cudaMalloc(&c->d_partial, sizeof(double) * 8 * kTotBlocksMax) != cudaSuccess ||
+      cudaMalloc(&c->d_tot, sizeof(double) * 8) != cudaSuccess || cudaMallocHost(&c->h_pin, 256) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking) != cudaSuccess) {
+    g_last_cuda = cudaGetErrorString(cudaGetLastError());
+    pmfmhd_destroy(c);
+    return PMFMHD_ENOMEM;
+  }
+  PMF_CK(cudaMemset(c->d_smax, 0, 256));
+  *out = c;
+  return PMFMHD_OK;
+}
+
+int pmfmhd_destroy(pmfmhd_ctx* c) {
+  if (c == nullptr) return PMFMHD_OK;
+  cudaSetDevice(c->device);
+  for (auto& e : c->graphs) cudaGraphExecDestroy(e.exec);
+  if (c->cap) cudaStreamDestroy(c->cap);
+  cudaFree(c->d_smax);
+  cudaFree(c->d_u64);
+  cudaFree(c->d_partial);
+  cudaFree(c->d_tot);
+  cudaFreeHost(c->h_pin);
+  delete c;
+  return PMFMHD_OK;
+}
+
+int pmfmhd_step_glm(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9], float dt,
+                    float ch, float decay, float* const resid[7], void* stream) {
+  if (c == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!nonnull(U, 9) || !nonnull(Unew, 9)) return PMFMHD_EINVAL;
+  if (!std::isfinite(dt) || !std::isfinite(ch) || !std::isfinite(decay) || !(ch > 0.0f)) return PMFMHD_EINVAL;
+  bool comp;
+  if ((rc = resid_mode(resid, &comp))) return rc;
+  return enqueue_glm(c, g, U, Unew, dt, ch, decay, resid, comp, as_stream(stream));
+}
+
+int pmfmhd_step_ct(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],
+                   float* ct_packed, float dt, float* const resid[7], int compensate_faces, void* stream) {
+  if (c == nullptr || ct_packed == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!all_periodic(g)) return PMFMHD_EUNSUPPORTED;
+  if (!nonnull(U, 9) || !nonnull(Unew, 9)) return PMFMHD_EINVAL;
+  if (!std::isfinite(dt)) return PMFMHD_EINVAL;
+  bool comp;
+  if ((rc = resid_mode(resid, &comp))) return rc;
+  return enqueue_ct(c, g, U, Unew, ct_packed, dt, resid, comp, compensate_faces != 0, as_stream(stream));
+}
+
+int pmfmhd_max_wavespeed(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* smax, void* stream) {
+  if (c == nullptr || smax == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!nonnull(U, 9)) return PMFMHD_EINVAL;
+  cudaStream_t s = as_stream(stream);
+  CPtr9 u;
+  for (int f = 0; f < 9; ++f) u.p[f] = U[f];
+  PMF_CK(cudaMemsetAsync(c->d_smax, 0, sizeof(unsigned int), s));
+  wavespeed_kernel<<<aux_blocks(c, ncells(g)), AUX_THREADS, 0, s>>>(u, (int)ncells(g), phys_of(g), c->d_smax);
+  PMF_CK(cudaGetLastError());
+  return read_smax(c, smax, s);
+}
+
+int pmfmhd_compute_dt(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float cfl, float* dt,
+                      float* smax, void* stream) {
+  if (dt == nullptr || !std::isfinite(cfl) || !(cfl > 0.0f)) return PMFMHD_EINVAL;
+  float sm;
+  int rc = pmfmhd_max_wavespeed(c, g, U, &sm, stream);
+  if (rc) return rc;
+  const float eps = 1.1920929e-7f;  // eps(Float32)
+  *dt = cfl * g->dx / (sm > eps ? sm : eps);  // timestep.jl:39
+  if (smax) *smax = sm;
+  return PMFMHD_OK;
+}
+
+int pmfmhd_last_wavespeed(pmfmhd_ctx* c, float* smax, void* stream) {
+  if (c == nullptr || smax == nullptr) return PMFMHD_EINVAL;
+  return read_smax(c, smax, as_stream(stream));
+}
+
+int pmfmhd_max_divb(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], double* out, void* stream) {
+  if (c == nullptr || out == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!nonnull(U, 9)) return PMFMHD_EINVAL;
+  cudaStream_t s = as_stream(stream);
+  PMF_CK(cudaMemsetAsync(c->d_u64, 0, sizeof(unsigned long long), s));
+  divb_kernel<<<aux_blocks(c, ncells(g)), AUX_THREADS, 0, s>>>(U[5], U[6], U[7], g->nx, g->ny, g->nz, g->bc[0],
+                                                                g->bc[1], g->bc[2], 1.0 / (2.0 * (double)g->dx),
+                                                                c->d_u64);
+  PMF_CK(cudaGetLastError());
+  PMF_CK(cudaMemcpyAsync(c->h_pin, c->d_u64, 8, cudaMemcpyDeviceToHost, s));
+  PMF_CK(cudaStreamSynchronize(s));
+  std::memcpy(out, c->h_pin, 8);
+  return PMFMHD_OK;
+}
+
+int pmfmhd_max_divb_face(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* ct, double* out, void* stream) {
+  if (c == nullptr || out == nullptr || ct == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  cudaStream_t s = as_stream(stream);
+  const long long nc = ncells(g);
+  PMF_CK(cudaMemsetAsync(c->d_u64, 0, sizeof(unsigned long long), s));
+  divb_face_kernel<<<aux_blocks(c, nc), AUX_THREADS, 0, s>>>(ct, ct + nc, ct + 2 * nc, g->nx, g->ny, g->nz,
+                                                              1.0 / (double)g->dx, c->d_u64);
+  PMF_CK(cudaGetLastError());
+  PMF_CK(cudaMemcpyAsync(c->h_pin, c->d_u64, 8, cudaMemcpyDeviceToHost, s));
+  PMF_CK(cudaStreamSynchronize(s));
+  std::memcpy(out, c->h_pin, 8);
+  return PMFMHD_OK;
+}
+
+int pmfmhd_conserved_totals(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], double out[8],
+                            void* stream) {
+  if (c == nullptr || out == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!nonnull(U, 9)) return PMFMHD_EINVAL;
+  cudaStream_t s = as_stream(stream);
+  CPtr9 u;
+  for (int f = 0; f < 9; ++f) u.p[f] = U[f];
+  const int nb = std::min(aux_blocks(c, ncells(g)), kTotBlocksMax);
+  totals_partial_kernel<<<nb, AUX_THREADS, 0, s>>>(u, (int)ncells(g), c->d_partial);
+  const float dV = g->dx * g->dx * g->dx;  // s.dx^3 in T (diagnostics.jl:45)
+  totals_final_kernel<<<1, 32, 0, s>>>(c->d_partial, nb, (double)dV, c->d_tot);
+  PMF_CK(cudaGetLastError());
+  PMF_CK(cudaMemcpyAsync(c->h_pin, c->d_tot, 64, cudaMemcpyDeviceToHost, s));
+  PMF_CK(cudaStreamSynchronize(s));
+  std::memcpy(out, c->h_pin, 64);
+  return PMFMHD_OK;
+}
+
+int pmfmhd_ct_faces_from_potential(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const A[3], float* const U[9],
+                                   float* ct, void* stream) {
+  if (c == nullptr || ct == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!all_periodic(g)) return PMFMHD_EUNSUPPORTED;
+  if (!nonnull(A, 3) || !nonnull(U, 9)) return PMFMHD_EINVAL;
+  cudaStream_t s = as_stream(stream);
+  const int nb = aux_blocks(c, ncells(g));
+  ct_curl_kernel<<<nb, AUX_THREADS, 0, s>>>(A[0], A[1], A[2], ct, g->nx, g->ny, g->nz, 1.0f / g->dx);
+  MPtr9 u;
+  for (int f = 0; f < 9; ++f) u.p[f] = U[f];
+  ct_cell_from_faces_kernel<<<nb, AUX_THREADS, 0, s>>>(ct, u, g->nx, g->ny, g->nz);
+  PMF_CK(cudaGetLastError());
+  return PMFMHD_OK;
+}
+
+int pmfmhd_run_glm(pmfmhd_ctx* c, const pmfmhd_grid* g, float* const U[9], float* const scratch[9], int nsteps,
+                   float dt, float ch, float decay, float* const resid[7], void* stream) {
+  if (c == nullptr || nsteps < 0) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!nonnull(U, 9) || !nonnull(scratch, 9)) return PMFMHD_EINVAL;
+  if (!std::isfinite(dt) || !std::isfinite(ch) || !std::isfinite(decay) || !(ch > 0.0f)) return PMFMHD_EINVAL;
+  bool comp;
+  if ((rc = resid_mode(resid, &comp))) return rc;
+  if (nsteps == 0) return PMFMHD_OK;
+  const Tune t = tune_for(c, g, false, comp);
+  // graph key: every input that changes the recorded launches
+  std::vector<unsigned char> key(sizeof(pmfmhd_grid) + 25 * sizeof(void*) + 3 * sizeof(float) + 3 * sizeof(int));
+  unsigned char* k = key.data();
+  std::memcpy(k, g, sizeof(pmfmhd_grid)); k += sizeof(pmfmhd_grid);
+  std::memcpy(k, U, 9 * sizeof(void*)); k += 9 * sizeof(void*);
+  std::memcpy(k, scratch, 9 * sizeof(void*)); k += 9 * sizeof(void*);
+  for (int i = 0; i < 7; ++i) {
+    void* p = comp ? (void*)resid[i] : nullptr;
+    std::memcpy(k, &p, sizeof(void*)); k += sizeof(void*);
+  }
+  std::memcpy(k, &dt, 4); k += 4;
+  std::memcpy(k, &ch, 4); k += 4;
+  std::memcpy(k, &decay, 4); k += 4;
+  std::memcpy(k, &nsteps, 4); k += 4;
+  std::memcpy(k, &t.ty, 4); k += 4;
+  std::memcpy(k, &t.tz, 4); k += 4;
+  cudaStream_t s = as_stream(stream);
+  std::lock_guard<std::mutex> lk(c->mu);
+  for (auto& e : c->graphs) {
+    if (e.key == key) {
+      PMF_CK(cudaGraphLaunch(e.exec, s));
+      return PMFMHD_OK;
+    }
+  }
+  // Record nsteps ping-pong steps on the capture stream, then replay on the caller's stream.
+  PMF_CK(cudaStreamBeginCapture(c->cap, cudaStreamCaptureModeThreadLocal));
+  const float dtdx = dt / g->dx;
+  for (int n = 0; n < nsteps; ++n) {
+    float* const* src = (n % 2 == 0) ? U : scratch;
+    float* const* dst = (n % 2 == 0) ? scratch : U;
+    StepArgs a;
+    fill_glm_args(a, src, dst, resid, comp, dtdx, ch, decay, c->d_smax);
+    cudaMemsetAsync(c->d_smax, 0, sizeof(unsigned int), c->cap);
+    int lrc = launch_step(g, a, t, false, comp, c->cap);
+    if (lrc != PMFMHD_OK) {
+      cudaGraph_t dead;
+      cudaStreamEndCapture(c->cap, &dead);
+      if (dead) cudaGraphDestroy(dead);
+      return lrc;
+    }
+  }
+  cudaGraph_t graph;
+  PMF_CK(cudaStreamEndCapture(c->cap, &graph));
+  cudaGraphExec_t exec;
+  cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    g_last_cuda = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+    return PMFMHD_ECUDA;
+  }
+  if (c->graphs.size() >= 16) {
+    cudaGraphExecDestroy(c->graphs.front().exec);
+    c->graphs.erase(c->graphs.begin());
+  }
+  c->graphs.push_back(GraphEntry{key, exec});
+  PMF_CK(cudaGraphLaunch(exec, s));
+  return PMFMHD_OK;
+}
+
+int pmfmhd_autotune(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], int mhd_solver, int compensated,
+                    void* stream) {
+  if (c == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!nonnull(U, 9)) return PMFMHD_EINVAL;
+  const bool ct = mhd_solver == 1;
+  if (ct && !all_periodic(g)) return PMFMHD_EUNSUPPORTED;
+  const bool comp = compensated != 0;
+  cudaStream_t s = as_stream(stream);
+  const long long nc = ncells(g);
+  // scratch copies so the caller's state is never touched
+  const size_t nfl = (size_t)nc * (9 + 9 + 7 + (ct ? CT_NSLOT : 0));
+  float* buf = nullptr;
+  if (cudaMalloc(&buf, nfl * sizeof(float)) != cudaSuccess) return PMFMHD_ENOMEM;
+  float* in[9];
+  float* outp[9];
+  float* res[7];
+  for (int f = 0; f < 9; ++f) { in[f] = buf + (size_t)f * nc; outp[f] = buf + (size_t)(9 + f) * nc; }
+  for (int i = 0; i < 7; ++i) res[i] = buf + (size_t)(18 + i) * nc;
+  float* ctp = ct ? buf + (size_t)25 * nc : nullptr;
+  int result = PMFMHD_OK;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int f = 0; f < 9 && result == PMFMHD_OK; ++f)
+    if (cudaMemcpyAsync(in[f], U[f], nc * sizeof(float), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      result = PMFMHD_ECUDA;
+  cudaMemsetAsync(res[0], 0, (size_t)7 * nc * sizeof(float), s);
+  if (ct) cudaMemsetAsync(ctp, 0, (size_t)CT_NSLOT * nc * sizeof(float), s);
+  Tune best = default_tune(c, g);
+  float best_ms = 1e30f;
+  std::vector<int> tzs = {g->nz, 256, 128, 64, 32, 16};
+  for (int ty : kTileRows) {
+    if (ty > 4 && g->ny < ty) continue;
+    for (int tz : tzs) {
+      if (tz > g->nz || tz < 1) continue;
+      Tune t{ty, tz};
+      float ms_sum = 0.0f;
+      for (int rep = 0; rep < 4 && result == PMFMHD_OK; ++rep) {
+        StepArgs a;
+        fill_glm_args(a, in, outp, res, comp, 1e-4f / g->dx, 1.0f, 1.0f, c->d_smax);
+        if (ct) {
+          for (int d = 0; d < 3; ++d) a.face[d] = ctp + (size_t)d * nc;
+          for (int k = 0; k < CT_NWORK; ++k) a.work[k] = ctp + (size_t)(CT_MFX + k) * nc;
+          a.smax_bits = nullptr;
+        }
+        cudaEventRecord(e0, s);
+        int lrc = launch_step(g, a, t, ct, comp, s);
+        cudaEventRecord(e1, s);
+        if (lrc != PMFMHD_OK) { result = lrc; break; }
+        if (cudaEventSynchronize(e1) != cudaSuccess) { result = PMFMHD_ECUDA; break; }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) ms_sum += ms;  // first launch is a warm-up
+      }
+      if (result != PMFMHD_OK) break;
+      if (ms_sum < best_ms) { best_ms = ms_sum; best = t; }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamSynchronize(s);
+  cudaFree(buf);
+  if (result == PMFMHD_OK) {
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->tune[TuneKey{g->nx, g->ny, g->nz, ct, comp, g->recon, g->riemann}] = best;
+  }
+  return result;
+}
+
+}  // extern "C"

@@ -1,0 +1,20 @@
+// Host-side view of the step-kernel instantiations.
+#pragma once
+#include <cstddef>
+
+namespace pmf {
+struct StepArgs;
+using StepKernel = void (*)(const StepArgs);
+
+struct StepKernelInfo {
+  StepKernel fn;      // null if the combination is not instantiated
+  size_t smem_bytes;  // dynamic shared memory per CTA
+  int threads;        // threads per CTA
+};
+
+// Rows per CTA that are instantiated (tile candidates for the autotuner).
+constexpr int kTileRows[] = {4, 8};
+constexpr int kNumTileRows = 2;
+
+StepKernelInfo step_kernel_info(int ty, int recon, int rsol, bool ct, bool comp);
+}  // namespace pmf

@@ -1,0 +1,380 @@
+// Fused MUSCL-Hancock Godunov step (GLM or CT Godunov stage) for sm_100a.
+//
+// Scheme: the reference's per-cell body (lib/MHDKernels/src/integrator_ref.jl:69-160, shared
+// with the shared-memory cube, integrator_cube.jl:295-444): MC-PLM/PPM/minmod offsets, the
+// multidimensional Hancock half step, one Riemann problem per face, and
+//   U' = U + dt/dx * (((Fxl-Fxh) + (Fyl-Fyh)) + (Fzl-Fzh)),  psi' *= decay.
+//
+// Decomposition (B200-specific, not the reference's 4^3 cube): one CTA owns a column of
+// 30 x TY cells in (x, y) and a chunk of planes in z, and marches through the chunk one
+// z-plane at a time.
+//   * warp w <-> row y0+w-1 (w = 0 and w = TY+1 are the y-halo rows); lane l <-> column
+//     x0+l-1 (lanes 0 and 31 are the x-halo cells). Each thread computes the Hancock state
+//     of its own cell once per plane.
+//   * x-faces are solved in registers: the left state comes from lane l-1 by __shfl_up,
+//     and the upper-face flux of a cell from lane l+1 by __shfl_down.
+//   * y-faces exchange one 9-float state per thread through shared memory.
+//   * z-faces never leave registers: each thread keeps the upper z-face state, the lower
+//     z-face flux and the x/y flux divergence of the previous plane of its own column, so
+//     plane p-1 is updated as soon as the z-face p-1/2 is solved in the pass over plane p.
+// Primitives of planes p-1, p, p+1 (with a 2-cell ring) live in a 3-slot shared ring; the
+// raw conserved plane p+2 is prefetched into a staging buffer by cp.async while plane p is
+// computed. Each face is solved exactly once per CTA; the only recomputation is the Hancock
+// state of the one-cell halo ring (~1.3x the owned cells) and the halo rows' y-faces.
+// The new state's max signal speed (timestep.jl:4-14) is reduced in the same pass.
+#pragma once
+#include "physics.cuh"
+
+namespace pmf {
+
+constexpr int TILE_X = 30;  // owned columns per CTA (32 lanes minus 2 halo lanes)
+constexpr int PLANE_W = 34; // primitive ring width: x0-2 .. x0+31
+
+// Number of CT workspace arrays written by the Godunov stage (reference CTState slots 4-15).
+constexpr int CT_NWORK = 12;
+
+struct StepArgs {
+  const float* U[9];
+  float* Un[9];
+  float* resid[7];          // compensated mode: remainders of mx, my, mz, E, Bx, By, Bz
+  const float* face[3];     // CT: lower-face normal B (bxf, byf, bzf)
+  float* work[CT_NWORK];    // CT: mfx mfy mfz fxby fxbz fybx fybz fzbx fzby ecx ecy ecz
+  int nx, ny, nz;
+  int bc[3];
+  int ntx, nty, nzc, tz;    // tiles along x, y; z chunks and planes per chunk
+  float dtdx, ch, decay;
+  Phys P;
+  unsigned int* smax_bits;  // fused CFL reduction target (bits of a non-negative float), or null
+  const float* dscal;       // if non-null: device {dtdx, ch, decay} overriding the values above
+};
+
+template <int TY>
+struct StepSmem {
+  static constexpr int PH = TY + 4;                 // rows y0-2 .. y0+TY+1
+  static constexpr int PP = PLANE_W * PH;           // cells per staged plane
+  static constexpr int STAGE = 9 * PP;              // raw conserved plane
+  static constexpr int PRIM = 3 * 9 * PP;           // 3-plane primitive ring
+  static constexpr int YB = (TY + 1) * 9 * 32;      // y-face states / fluxes
+  static constexpr int FLOATS = STAGE + PRIM + 2 * YB;
+  static constexpr size_t BYTES = sizeof(float) * FLOATS;
+};
+
+__device__ __forceinline__ void cp_async4(float* smem_dst, const float* gsrc) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+template <int TY, int RECON, int RSOL, bool CT, bool COMP>
+__global__ void __launch_bounds__(32 * (TY + 2), 1) mhd_step_kernel(const StepArgs a) {
+  using S = StepSmem<TY>;
+  constexpr int NT = 32 * (TY + 2);
+  constexpr int PP = S::PP;
+  extern __shared__ float smem[];
+  float* stage = smem;
+  float* prim = smem + S::STAGE;
+  float* ybuf = prim + S::PRIM;
+  float* fybuf = ybuf + S::YB;
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, w = tid >> 5;
+  const int bid = blockIdx.x;
+  const int tx = bid % a.ntx, ty = (bid / a.ntx) % a.nty, zc = bid / (a.ntx * a.nty);
+  const int x0 = tx * TILE_X, y0 = ty * TY;
+  const int z0 = zc * a.tz;
+  const int z1 = min(z0 + a.tz, a.nz);
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int nxy = nx * ny;
+
+  float dtdx = a.dtdx, ch = a.ch, decay = a.decay;
+  if (a.dscal != nullptr) { dtdx = a.dscal[0]; ch = a.dscal[1]; decay = a.dscal[2]; }
+  const Phys P = a.P;
+  const float g = P.gamma;
+
+  const int x = x0 + lane - 1, y = y0 + w - 1;
+  const bool own = lane >= 1 && lane <= TILE_X && w >= 1 && w <= TY && x < nx && y < ny;
+  const bool row_own = w >= 1 && w <= TY;
+
+  // Source cell of staged-plane entry e (row r, column c) of logical plane zp, with BCs.
+  auto issue_plane = [&](int zp) {
+    float fz;
+    const int kz = bc_index(zp, nz, a.bc[2], &fz);
+    for (int e = tid; e < PP; e += NT) {
+      const int r = e / PLANE_W, c = e - r * PLANE_W;
+      float fx, fy;
+      const int ix = bc_index(x0 + c - 2, nx, a.bc[0], &fx);
+      const int iy = bc_index(y0 + r - 2, ny, a.bc[1], &fy);
+      const int gi = kz * nxy + iy * nx + ix;
+#pragma unroll
+      for (int f = 0; f < 9; ++f) cp_async4(stage + f * PP + e, a.U[f] + gi);
+    }
+    cp_async_commit();
+  };
+  // Raw conserved -> primitive (reflecting walls flip the normal components first).
+  auto convert_plane = [&](int zp, float* dst) {
+    float fz;
+    bc_index(zp, nz, a.bc[2], &fz);
+    for (int e = tid; e < PP; e += NT) {
+      const int r = e / PLANE_W, c = e - r * PLANE_W;
+      float fx, fy;
+      bc_index(x0 + c - 2, nx, a.bc[0], &fx);
+      bc_index(y0 + r - 2, ny, a.bc[1], &fy);
+      F9 u;
+#pragma unroll
+      for (int f = 0; f < 9; ++f) u[f] = stage[f * PP + e];
+      u[1] *= fx; u[5] *= fx;
+      u[2] *= fy; u[6] *= fy;
+      u[3] *= fz; u[7] *= fz;
+      F9 q = cons2prim(u, g, P.smallr, P.pfl);
+#pragma unroll
+      for (int f = 0; f < 9; ++f) dst[f * PP + e] = q[f];
+    }
+  };
+  auto slot = [&](int zp) { return prim + ((zp - z0 + 3) % 3) * (9 * PP); };
+  auto ld9 = [&](const float* pl, int r, int c) {
+    F9 q;
+#pragma unroll
+    for (int f = 0; f < 9; ++f) q[f] = pl[f * PP + r * PLANE_W + c];
+    return q;
+  };
+
+  // Prologue: primitives of planes z0-2 and z0-1, plane z0 in flight.
+  issue_plane(z0 - 2);
+  cp_async_wait_all();
+  __syncthreads();
+  convert_plane(z0 - 2, slot(z0 - 2));
+  __syncthreads();
+  issue_plane(z0 - 1);
+  cp_async_wait_all();
+  __syncthreads();
+  convert_plane(z0 - 1, slot(z0 - 1));
+  __syncthreads();
+  issue_plane(z0);
+
+  // Per-column carries across planes.
+  F9 zR;      // upper z-face state of plane p-1
+  F9 Fzc;     // flux through the lower z-face of plane p-1
+  F9 dUxy;    // (Fxl - Fxh) + (Fyl - Fyh) of plane p-1
+  float smax = 0.0f;
+  const int r0 = w + 1, c0 = lane + 1;  // this thread's cell in the staged plane
+
+  for (int p = z0 - 1; p <= z1; ++p) {
+    cp_async_wait_all();
+    __syncthreads();
+    convert_plane(p + 1, slot(p + 1));
+    __syncthreads();
+    if (p + 2 <= z1 + 1) issue_plane(p + 2);
+
+    // ---- Hancock half step of this thread's cell in plane p ------------------------------
+    const float* pm = slot(p - 1);
+    const float* p0 = slot(p);
+    const float* pp = slot(p + 1);
+    const F9 m0 = ld9(p0, r0, c0);
+    const Offsets<RECON> ox = recon<RECON>(ld9(p0, r0, c0 - 1), m0, ld9(p0, r0, c0 + 1));
+    const Offsets<RECON> oy = recon<RECON>(ld9(p0, r0 - 1, c0), m0, ld9(p0, r0 + 1, c0));
+    const Offsets<RECON> oz = recon<RECON>(ld9(pm, r0, c0), m0, ld9(pp, r0, c0));
+    F9 mh;
+    {
+      const F9 u0 = prim2cons(m0, g);
+      F9 acc = hancock_term<0, RECON>(m0, ox, g);
+      acc = add9(acc, hancock_term<1, RECON>(m0, oy, g));
+      acc = add9(acc, hancock_term<2, RECON>(m0, oz, g));
+      const float h = 0.5f * dtdx;
+      F9 uh;
+#pragma unroll
+      for (int i = 0; i < 9; ++i) uh[i] = u0[i] - h * acc[i];
+      mh = cons2prim(uh, g, P.smallr, P.pfl);
+    }
+    const int cell_p = (p >= 0 && p < nz && x < nx && y < ny) ? (p * nxy + y * nx + x) : 0;
+
+    if (p == z0 - 1) {
+      zR = face_hi<RECON>(mh, oz);
+      continue;
+    }
+
+    F9 Fz;
+    {
+      // z-face p-1/2: left = upper z state of plane p-1 (carried), right = lower z state of p
+      F9 L = zR, R = face_lo<RECON>(mh, oz);
+      if constexpr (CT) {
+        float zf;
+        const int kz = bc_index(p, nz, BC_PERIODIC, &zf);
+        float xf, yf;
+        const int ix = bc_index(x, nx, BC_PERIODIC, &xf), iy = bc_index(y, ny, BC_PERIODIC, &yf);
+        const float bn = __ldg(a.face[2] + kz * nxy + iy * nx + ix);
+        L[7] = bn; R[7] = bn;
+      }
+      Fz = riemann<2, RSOL, CT>(L, R, ch, P);
+    }
+
+    if (p < z1) {
+      // ---- x-faces: lane l solves the face between cells l-1 and l ------------------------
+      F9 dx_flux;  // (Fxl - Fxh) for this cell
+      F9 Fx;
+      if (row_own) {
+        F9 L, R = face_lo<RECON>(mh, ox);
+        const F9 xR = face_hi<RECON>(mh, ox);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) L[i] = __shfl_up_sync(0xffffffffu, xR[i], 1);
+        if constexpr (CT) {
+          float f0;
+          const int ix = bc_index(x, nx, BC_PERIODIC, &f0);
+          const int iy = bc_index(y, ny, BC_PERIODIC, &f0);
+          const int kz = bc_index(p, nz, BC_PERIODIC, &f0);
+          const float bn = __ldg(a.face[0] + kz * nxy + iy * nx + ix);
+          L[5] = bn; R[5] = bn;
+        }
+        Fx = riemann<0, RSOL, CT>(L, R, ch, P);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) dx_flux[i] = Fx[i] - __shfl_down_sync(0xffffffffu, Fx[i], 1);
+      }
+      // ---- y-faces: rows 0..TY publish their upper y state; rows 1..TY+1 solve ------------
+      if (w <= TY) {
+        const F9 yR = face_hi<RECON>(mh, oy);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) ybuf[(w * 9 + i) * 32 + lane] = yR[i];
+      }
+      __syncthreads();
+      F9 Fy;
+      if (w >= 1) {
+        F9 L, R = face_lo<RECON>(mh, oy);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) L[i] = ybuf[((w - 1) * 9 + i) * 32 + lane];
+        if constexpr (CT) {
+          float f0;
+          const int ix = bc_index(x, nx, BC_PERIODIC, &f0);
+          const int iy = bc_index(y, ny, BC_PERIODIC, &f0);
+          const int kz = bc_index(p, nz, BC_PERIODIC, &f0);
+          const float bn = __ldg(a.face[1] + kz * nxy + iy * nx + ix);
+          L[6] = bn; R[6] = bn;
+        }
+        Fy = riemann<1, RSOL, CT>(L, R, ch, P);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) fybuf[((w - 1) * 9 + i) * 32 + lane] = Fy[i];
+      }
+      __syncthreads();
+      F9 dUxy_p;
+      if (row_own) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) dUxy_p[i] = dx_flux[i] + (Fy[i] - fybuf[(w * 9 + i) * 32 + lane]);
+      }
+      if constexpr (CT) {
+        // lower-face fluxes and the cell-centred reference EMF -v x B (v of the predicted
+        // state, B at the start of the step) for the edge EMFs (integrator_ref.jl:127-139)
+        if (own) {
+          a.work[0][cell_p] = Fx[0];
+          a.work[1][cell_p] = Fy[0];
+          a.work[2][cell_p] = Fz[0];
+          a.work[3][cell_p] = Fx[6];
+          a.work[4][cell_p] = Fx[7];
+          a.work[5][cell_p] = Fy[5];
+          a.work[6][cell_p] = Fy[7];
+          a.work[7][cell_p] = Fz[5];
+          a.work[8][cell_p] = Fz[6];
+          a.work[9][cell_p] = mh[3] * m0[6] - mh[2] * m0[7];
+          a.work[10][cell_p] = mh[1] * m0[7] - mh[3] * m0[5];
+          a.work[11][cell_p] = mh[2] * m0[5] - mh[1] * m0[6];
+        }
+      }
+      if (p > z0) {
+        // update plane p-1 with its carried x/y divergence and its two z fluxes
+        if (own) {
+          const int c = (p - 1) * nxy + y * nx + x;
+          F9 u0;
+#pragma unroll
+          for (int f = 0; f < 9; ++f) u0[f] = __ldg(a.U[f] + c);
+          F9 un;
+          float d[9];
+#pragma unroll
+          for (int i = 0; i < 9; ++i) d[i] = dtdx * (dUxy[i] + (Fzc[i] - Fz[i]));
+          un[0] = u0[0] + d[0];
+          if constexpr (COMP) {
+#pragma unroll
+            for (int i = 1; i <= 4; ++i) {
+              float r = a.resid[i - 1][c];
+              un[i] = comp_add(u0[i], d[i], r);
+              a.resid[i - 1][c] = r;
+            }
+            if constexpr (!CT) {
+#pragma unroll
+              for (int i = 5; i <= 7; ++i) {
+                float r = a.resid[i - 1][c];
+                un[i] = comp_add(u0[i], d[i], r);
+                a.resid[i - 1][c] = r;
+              }
+            }
+          } else {
+#pragma unroll
+            for (int i = 1; i <= 7; ++i) un[i] = u0[i] + d[i];
+          }
+          un[8] = CT ? 0.0f : (u0[8] + d[8]) * decay;
+#pragma unroll
+          for (int f = 0; f < 9; ++f) {
+            if (CT && f >= 5 && f <= 7) continue;  // cell B comes from the face average
+            a.Un[f][c] = un[f];
+          }
+          if (!CT && a.smax_bits != nullptr) smax = fmaxf(smax, cell_wavespeed(un, P));
+        }
+      }
+      if (row_own) dUxy = dUxy_p;
+      zR = face_hi<RECON>(mh, oz);
+      Fzc = Fz;
+    } else {
+      // p == z1: only the z-face z1-1/2 is needed; update the last owned plane.
+      if (own) {
+        const int c = (p - 1) * nxy + y * nx + x;
+        F9 u0;
+#pragma unroll
+        for (int f = 0; f < 9; ++f) u0[f] = __ldg(a.U[f] + c);
+        F9 un;
+        float d[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) d[i] = dtdx * (dUxy[i] + (Fzc[i] - Fz[i]));
+        un[0] = u0[0] + d[0];
+        if constexpr (COMP) {
+#pragma unroll
+          for (int i = 1; i <= 4; ++i) {
+            float r = a.resid[i - 1][c];
+            un[i] = comp_add(u0[i], d[i], r);
+            a.resid[i - 1][c] = r;
+          }
+          if constexpr (!CT) {
+#pragma unroll
+            for (int i = 5; i <= 7; ++i) {
+              float r = a.resid[i - 1][c];
+              un[i] = comp_add(u0[i], d[i], r);
+              a.resid[i - 1][c] = r;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int i = 1; i <= 7; ++i) un[i] = u0[i] + d[i];
+        }
+        un[8] = CT ? 0.0f : (u0[8] + d[8]) * decay;
+#pragma unroll
+        for (int f = 0; f < 9; ++f) {
+          if (CT && f >= 5 && f <= 7) continue;
+          a.Un[f][c] = un[f];
+        }
+        if (!CT && a.smax_bits != nullptr) smax = fmaxf(smax, cell_wavespeed(un, P));
+      }
+    }
+  }
+  cp_async_wait_all();
+
+  if (!CT && a.smax_bits != nullptr) {
+    __shared__ float red[32];
+    __syncthreads();
+    float m = warp_max(smax);
+    if (lane == 0) red[w] = m;
+    __syncthreads();
+    if (w == 0) {
+      m = lane < (NT / 32) ? red[lane] : 0.0f;
+      m = warp_max(m);
+      if (lane == 0) atomicMax(a.smax_bits, __float_as_uint(m));
+    }
+  }
+}
+
+}  // namespace pmf

@@ -1,0 +1,491 @@
+"""Host-side mirror of MHDKernels' step API over libpmfmhd.so (ctypes; torch owns memory).
+
+The names, arguments and error behaviour follow lib/MHDKernels/src: ``allocate_state``
+(state.jl:123-141), ``step`` / ``step_cube`` / ``step_ref`` (driver.jl:20-37,
+integrator_cube.jl:455-463, integrator_ref.jl:210-220), ``evolve`` (driver.jl:48-71),
+``compute_dt`` / ``max_wavespeed`` (timestep.jl:17-46), ``max_divb`` /
+``conserved_totals`` (diagnostics.jl:22-55), ``max_divb_face`` / ``ct_faces_from_potential``
+/ ``ct_faces_from_cells`` (ct.jl:187-345). Errors raise ``PMFMHDError`` where the
+reference calls ``error(...)``. Every step runs the sm_100a CUDA library; there is no CPU
+path, and a missing library raises at import of the first call.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpmfmhd.so")
+
+GLM_CR = 0.18  # driver.jl:8
+NVAR = 9
+RECON = {"plm": 0, "ppm": 1, "plm_minmod": 2}
+RIEMANN = {"hlld": 0, "hll": 1, "llf": 2}
+BC = {"periodic": 0, "outflow": 1, "reflecting": 2}
+CT_NSLOT = 21
+FLOAT32_EPS = float(np.finfo(np.float32).eps)
+
+
+class PMFMHDError(RuntimeError):
+    pass
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+                ("bc", ctypes.c_int32 * 3), ("recon", ctypes.c_int32), ("riemann", ctypes.c_int32),
+                ("dx", ctypes.c_float), ("gamma", ctypes.c_float), ("smallr", ctypes.c_float),
+                ("pfl", ctypes.c_float), ("llf_dmin", ctypes.c_float), ("llf_pmin", ctypes.c_float)]
+
+
+class Box(ctypes.Structure):
+    _fields_ = [("grid", Grid), ("U", ctypes.c_void_p * 9), ("scratch", ctypes.c_void_p * 9),
+                ("ct_packed", ctypes.c_void_p), ("resid", ctypes.c_void_p * 7), ("mhd_solver", ctypes.c_int32),
+                ("cfl", ctypes.c_float), ("glm_ch_fac", ctypes.c_float), ("glm_cr", ctypes.c_float)]
+
+
+# Exported symbols and their signatures (include/pmfmhd.h).
+_VP = ctypes.c_void_p
+_P9 = ctypes.c_void_p * 9
+_P7 = ctypes.c_void_p * 7
+_P3 = ctypes.c_void_p * 3
+_GP = ctypes.POINTER(Grid)
+SIGNATURES = {
+    "pmfmhd_version": ([], ctypes.c_int),
+    "pmfmhd_strerror": ([ctypes.c_int], ctypes.c_char_p),
+    "pmfmhd_last_cuda_error": ([], ctypes.c_char_p),
+    "pmfmhd_create": ([ctypes.c_int, ctypes.POINTER(_VP)], ctypes.c_int),
+    "pmfmhd_destroy": ([_VP], ctypes.c_int),
+    "pmfmhd_step_glm": ([_VP, _GP, _P9, _P9, ctypes.c_float, ctypes.c_float, ctypes.c_float, _VP, _VP], ctypes.c_int),
+    "pmfmhd_step_ct": ([_VP, _GP, _P9, _P9, _VP, ctypes.c_float, _VP, ctypes.c_int, _VP], ctypes.c_int),
+    "pmfmhd_max_wavespeed": ([_VP, _GP, _P9, ctypes.POINTER(ctypes.c_float), _VP], ctypes.c_int),
+    "pmfmhd_compute_dt": ([_VP, _GP, _P9, ctypes.c_float, ctypes.POINTER(ctypes.c_float),
+                           ctypes.POINTER(ctypes.c_float), _VP], ctypes.c_int),
+    "pmfmhd_last_wavespeed": ([_VP, ctypes.POINTER(ctypes.c_float), _VP], ctypes.c_int),
+    "pmfmhd_max_divb": ([_VP, _GP, _P9, ctypes.POINTER(ctypes.c_double), _VP], ctypes.c_int),
+    "pmfmhd_max_divb_face": ([_VP, _GP, _VP, ctypes.POINTER(ctypes.c_double), _VP], ctypes.c_int),
+    "pmfmhd_conserved_totals": ([_VP, _GP, _P9, ctypes.c_double * 8, _VP], ctypes.c_int),
+    "pmfmhd_ct_faces_from_potential": ([_VP, _GP, _P3, _P9, _VP, _VP], ctypes.c_int),
+    "pmfmhd_run_glm": ([_VP, _GP, _P9, _P9, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, _VP, _VP],
+                       ctypes.c_int),
+    "pmfmhd_batch_create": ([_VP, ctypes.POINTER(Box), ctypes.c_int, ctypes.POINTER(_VP)], ctypes.c_int),
+    "pmfmhd_batch_step": ([_VP, ctypes.c_int, _VP], ctypes.c_int),
+    "pmfmhd_batch_query": ([_VP, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32),
+                            ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
+    "pmfmhd_batch_destroy": ([_VP], ctypes.c_int),
+    "pmfmhd_autotune": ([_VP, _GP, _P9, ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
+}
+
+_lib = None
+_ctx = {}
+
+
+def lib():
+    """Load libpmfmhd.so; raise if it has not been built (there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise PMFMHDError(f"libpmfmhd.so not built at {LIB_PATH}; run `make -C {HERE}`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (argtypes, restype) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = argtypes
+            f.restype = restype
+        _lib = L
+    return _lib
+
+
+def _check(rc, what):
+    if rc != 0:
+        L = lib()
+        msg = L.pmfmhd_strerror(rc).decode()
+        cuda = L.pmfmhd_last_cuda_error().decode()
+        raise PMFMHDError(f"{what}: {msg} (code {rc})" + (f": {cuda}" if cuda and rc == -3 else ""))
+
+
+def context(device: Optional[int] = None):
+    """Per-device library context (reduction workspace, tile table, cached graphs)."""
+    if device is None:
+        device = torch.cuda.current_device()
+    if device not in _ctx:
+        if not torch.cuda.is_available():
+            raise PMFMHDError("no CUDA device: libpmfmhd needs an sm_100a GPU")
+        h = _VP()
+        with torch.cuda.device(device):
+            _check(lib().pmfmhd_create(device, ctypes.byref(h)), "pmfmhd_create")
+        _ctx[device] = h
+    return _ctx[device]
+
+
+def _stream():
+    return _VP(torch.cuda.current_stream().cuda_stream)
+
+
+def _p9(ts) -> "ctypes.Array":
+    return _P9(*[t.data_ptr() for t in ts])
+
+
+@dataclass
+class CTState:
+    """Reference CTState (state.jl:44-58): one packed buffer of 21 slots of ncells."""
+    packed: torch.Tensor
+    nc: int
+
+    def slot(self, q: int) -> torch.Tensor:
+        return self.packed[q * self.nc:(q + 1) * self.nc]
+
+    @property
+    def bxf(self): return self.slot(0)
+    @property
+    def byf(self): return self.slot(1)
+    @property
+    def bzf(self): return self.slot(2)
+    @property
+    def rbx(self): return self.slot(18)
+    @property
+    def rby(self): return self.slot(19)
+    @property
+    def rbz(self): return self.slot(20)
+
+
+@dataclass
+class MHDState:
+    U: list
+    scratch: list
+    dims: tuple
+    dx: float
+    gamma: float
+    smallr: float
+    pfl: float
+    llf_dmin: float
+    llf_pmin: float
+    riemann: str
+    recon: str
+    bcs: tuple
+    device: int
+    ct: Optional[CTState] = None
+    resid: Optional[list] = None
+    grid: Grid = field(default=None, repr=False)
+
+    @property
+    def nc(self):
+        return int(np.prod(self.dims))
+
+    def uses_ct(self):
+        return self.ct is not None
+
+    def mhd_solver(self):
+        return "ct" if self.ct is not None else "glm"
+
+
+def uses_ct(s: MHDState) -> bool:
+    return s.ct is not None
+
+
+def allocate_state(dims: Sequence[int], dx: float, gamma: float = 5 / 3, smallr: float = 1e-6, pfl: float = 1e-7,
+                   llf_dmin: float = 1e-4, llf_pmin: float = 0.0, use_hlld: bool = True, riemann=None,
+                   bc: str = "periodic", bcs=None, recon: str = "plm", mhd_solver: str = "glm",
+                   compensated: bool = False, device: Optional[int] = None) -> MHDState:
+    """Zero-filled FP32 state on the GPU (state.jl:123-141). ``compensated`` adds the seven
+    Kahan remainder arrays of the compensated update (momentum, E, B)."""
+    if mhd_solver not in ("glm", "ct"):
+        raise PMFMHDError(f"unknown mhd_solver :{mhd_solver} (have :glm, :ct)")
+    bcs = tuple(bcs) if bcs is not None else (bc, bc, bc)
+    for b in bcs:
+        if b not in BC:
+            raise PMFMHDError(f"unknown BC :{b} (have :periodic, :outflow, :reflecting)")
+    if mhd_solver == "ct" and any(b != "periodic" for b in bcs):
+        raise PMFMHDError(f"mhd_solver=:ct requires all-periodic boundaries (bcs={bcs}); "
+                          "constrained transport is periodic-only")
+    rsym = riemann if riemann is not None else ("hlld" if use_hlld else "llf")
+    if rsym not in RIEMANN:
+        raise PMFMHDError(f"unknown MHD riemann :{rsym} (have :hlld, :hll, :llf)")
+    if recon not in RECON:
+        raise PMFMHDError(f"unknown recon :{recon} (have :plm, :plm_minmod, :ppm)")
+    if device is None:
+        device = torch.cuda.current_device()
+    dims = tuple(int(d) for d in dims)
+    nc = int(np.prod(dims))
+    dev = torch.device("cuda", device)
+    U = [torch.zeros(nc, dtype=torch.float32, device=dev) for _ in range(NVAR)]
+    sc = [torch.zeros(nc, dtype=torch.float32, device=dev) for _ in range(NVAR)]
+    ct = CTState(torch.zeros(CT_NSLOT * nc, dtype=torch.float32, device=dev), nc) if mhd_solver == "ct" else None
+    resid = [torch.zeros(nc, dtype=torch.float32, device=dev) for _ in range(7)] if compensated else None
+    f32 = lambda v: float(np.float32(v))
+    s = MHDState(U, sc, dims, f32(dx), f32(gamma), f32(smallr), f32(pfl), f32(llf_dmin), f32(llf_pmin), rsym, recon,
+                 bcs, device, ct, resid)
+    s.grid = Grid(dims[0], dims[1], dims[2], (ctypes.c_int32 * 3)(*[BC[b] for b in bcs]), RECON[recon],
+                  RIEMANN[rsym], s.dx, s.gamma, s.smallr, s.pfl, s.llf_dmin, s.llf_pmin)
+    return s
+
+
+def set_fields(s: MHDState, U_host) -> MHDState:
+    """Copy a host ``(9, nc)`` conserved array into the state."""
+    U_host = np.ascontiguousarray(np.asarray(U_host, dtype=np.float32).reshape(NVAR, s.nc))
+    for v in range(NVAR):
+        s.U[v].copy_(torch.from_numpy(U_host[v]))
+    return s
+
+
+def fields_to_host(s: MHDState) -> np.ndarray:
+    """``(9, nc)`` host copy of the conserved fields (state.jl:143-144)."""
+    return torch.stack(s.U).cpu().numpy()
+
+
+def _resid_arg(s: MHDState):
+    return _P7(*[t.data_ptr() for t in s.resid]) if s.resid is not None else None
+
+
+def step_cube(s: MHDState, dt: float, ch: float, decay: float) -> MHDState:
+    """One GLM step into the scratch set, then swap (integrator_cube.jl:455-463)."""
+    if uses_ct(s):
+        raise PMFMHDError("step_cube!: CT is implemented on the :ref integrator only "
+                          "(mhd_solver=:ct states cannot use the :cube integrators)")
+    _check(lib().pmfmhd_step_glm(context(s.device), ctypes.byref(s.grid), _p9(s.U), _p9(s.scratch), float(dt),
+                                 float(ch), float(decay), _resid_arg(s), _stream()), "step_cube!")
+    s.U, s.scratch = s.scratch, s.U
+    return s
+
+
+def step_ref(s: MHDState, dt: float, ch: float, decay: float, compensate_faces: bool = False) -> MHDState:
+    """integrator_ref.jl:210-220 (+ ct_update!): the same fused kernel; CT states run the
+    Godunov stage and the CT face update."""
+    if uses_ct(s):
+        _check(lib().pmfmhd_step_ct(context(s.device), ctypes.byref(s.grid), _p9(s.U), _p9(s.scratch),
+                                    s.ct.packed.data_ptr(), float(dt), _resid_arg(s), int(compensate_faces),
+                                    _stream()), "step_ref!")
+        s.U, s.scratch = s.scratch, s.U
+        return s
+    return step_cube(s, dt, ch, decay)
+
+
+def step(s: MHDState, dt: float, ch: Optional[float] = None, glm_cr: float = GLM_CR,
+         integrator: str = "cube") -> MHDState:
+    """driver.jl:20-37. CT states ignore ``ch``/``glm_cr``."""
+    if integrator not in ("ref", "cube"):
+        raise PMFMHDError(f"unknown integrator :{integrator} (have :ref, :cube)")
+    if uses_ct(s):
+        if integrator != "ref":
+            raise PMFMHDError("step!: CT is implemented on the :ref integrator only "
+                              "(mhd_solver=:ct states cannot use the :cube integrators)")
+        return step_ref(s, dt, 0.0, 1.0)
+    if ch is None:
+        raise PMFMHDError("step! needs the GLM cleaning speed `ch` (GLM states)")
+    T = np.float32
+    decay = float(np.exp(T(T(-T(glm_cr) * T(ch) * T(dt)) / T(s.dx))))
+    return step_cube(s, dt, ch, decay)
+
+
+def max_wavespeed(s: MHDState) -> float:
+    out = ctypes.c_float()
+    _check(lib().pmfmhd_max_wavespeed(context(s.device), ctypes.byref(s.grid), _p9(s.U), ctypes.byref(out),
+                                      _stream()), "max_wavespeed")
+    return out.value
+
+
+def compute_dt(s: MHDState, cfl: float = 0.4):
+    """(dt, smax) with dt = cfl*dx/max(smax, eps) (timestep.jl:37-46)."""
+    dt, smax = ctypes.c_float(), ctypes.c_float()
+    _check(lib().pmfmhd_compute_dt(context(s.device), ctypes.byref(s.grid), _p9(s.U), float(cfl), ctypes.byref(dt),
+                                   ctypes.byref(smax), _stream()), "compute_dt")
+    return dt.value, smax.value
+
+
+def last_wavespeed(s: MHDState) -> float:
+    out = ctypes.c_float()
+    _check(lib().pmfmhd_last_wavespeed(context(s.device), ctypes.byref(out), _stream()), "last_wavespeed")
+    return out.value
+
+
+def evolve(s: MHDState, tfinal: float, cfl: float = 0.4, glm_ch_fac: float = 1.0, glm_cr: float = GLM_CR,
+           integrator: Optional[str] = None, callback=None):
+    """driver.jl:48-71: CFL-limited steps to ``tfinal``; returns (t, nsteps)."""
+    if not glm_ch_fac > 0:
+        raise PMFMHDError("glm_ch_fac must be positive")
+    if not glm_cr >= 0:
+        raise PMFMHDError("glm_cr must be non-negative")
+    if integrator is None:
+        integrator = "ref" if uses_ct(s) else "cube"
+    T = np.float32
+    t, n, tf = 0.0, 0, float(tfinal)
+    while t < tf * (1 - 1e-9):
+        dt, smax = compute_dt(s, cfl)
+        if uses_ct(s):
+            ch = T(0)
+            dtf = float(dt)
+        else:
+            ch = T(T(glm_ch_fac) * T(smax))
+            dtf = float(dt) * float(smax) / float(max(T(smax), ch))
+        if t + dtf > tf:
+            dtf = tf - t
+        step(s, dtf, ch=float(ch), glm_cr=glm_cr, integrator=integrator)
+        t += dtf
+        n += 1
+        if callback is not None:
+            callback(s, t, n)
+    return t, n
+
+
+def run_glm(s: MHDState, nsteps: int, dt: float, ch: float, decay: float) -> MHDState:
+    """nsteps fixed-dt GLM steps replayed from a cached CUDA graph; the state ends in s.U."""
+    _check(lib().pmfmhd_run_glm(context(s.device), ctypes.byref(s.grid), _p9(s.U), _p9(s.scratch), int(nsteps),
+                                float(dt), float(ch), float(decay), _resid_arg(s), _stream()), "run_glm")
+    if nsteps % 2 == 1:
+        s.U, s.scratch = s.scratch, s.U
+    return s
+
+
+def autotune(s: MHDState) -> None:
+    _check(lib().pmfmhd_autotune(context(s.device), ctypes.byref(s.grid), _p9(s.U), 1 if uses_ct(s) else 0,
+                                 1 if s.resid is not None else 0, _stream()), "autotune")
+
+
+def max_divb(s: MHDState) -> float:
+    out = ctypes.c_double()
+    _check(lib().pmfmhd_max_divb(context(s.device), ctypes.byref(s.grid), _p9(s.U), ctypes.byref(out), _stream()),
+           "max_divb")
+    return out.value
+
+
+def max_divb_face(s: MHDState) -> float:
+    if not uses_ct(s):
+        raise PMFMHDError("max_divb_face needs a CT state (mhd_solver=:ct)")
+    out = ctypes.c_double()
+    _check(lib().pmfmhd_max_divb_face(context(s.device), ctypes.byref(s.grid), s.ct.packed.data_ptr(),
+                                      ctypes.byref(out), _stream()), "max_divb_face")
+    return out.value
+
+
+def conserved_totals(s: MHDState) -> dict:
+    out = (ctypes.c_double * 8)()
+    _check(lib().pmfmhd_conserved_totals(context(s.device), ctypes.byref(s.grid), _p9(s.U), out, _stream()),
+           "conserved_totals")
+    keys = ("mass", "momx", "momy", "momz", "energy", "Bx", "By", "Bz")
+    return dict(zip(keys, list(out)))
+
+
+def ct_faces_from_potential(s: MHDState, Ax, Ay, Az) -> MHDState:
+    """ct.jl:332-345: faces = discrete curl of an edge potential, cell B = face average."""
+    if not uses_ct(s):
+        raise PMFMHDError("ct_faces_from_potential! needs a CT state (mhd_solver=:ct)")
+    dev = torch.device("cuda", s.device)
+    A = []
+    for a in (Ax, Ay, Az):
+        a = torch.as_tensor(np.asarray(a, dtype=np.float32).reshape(-1) if not torch.is_tensor(a) else a)
+        if a.numel() != s.nc:
+            raise PMFMHDError(f"vector-potential array has {a.numel()} entries, expected {s.nc}")
+        A.append(a.to(dev, torch.float32).contiguous())
+    _check(lib().pmfmhd_ct_faces_from_potential(context(s.device), ctypes.byref(s.grid),
+                                                _P3(*[a.data_ptr() for a in A]), _p9(s.U), s.ct.packed.data_ptr(),
+                                                _stream()), "ct_faces_from_potential!")
+    torch.cuda.current_stream().synchronize()
+    return s
+
+
+def ct_faces_from_cells(s: MHDState) -> dict:
+    """ct.jl:246-308: project the cell B onto the CT-admissible subspace (host FP64 FFT),
+    install faces, cell B = face average, E keeps the thermal pressure, psi = 0."""
+    if not uses_ct(s):
+        raise PMFMHDError("ct_faces_from_cells! needs a CT state (mhd_solver=:ct)")
+    nx, ny, nz = s.dims
+    h = fields_to_host(s).astype(np.float64)
+    Bold = [h[5 + d].reshape(nz, ny, nx) for d in range(3)]
+    Bh = [np.fft.rfftn(b) for b in Bold]  # axes (z, y, x); rfft along x
+
+    def half_phase(n, m):
+        mm = np.where(m > n / 2, m - n, m)
+        nyq = (n % 2 == 0) & (m == n // 2)
+        return np.where(nyq, 0.0, np.pi * mm / n), nyq
+
+    tx, nqx = half_phase(nx, np.arange(nx // 2 + 1))
+    ty, nqy = half_phase(ny, np.arange(ny))
+    tz, nqz = half_phase(nz, np.arange(nz))
+    thz, thy, thx = np.meshgrid(tz, ty, tx, indexing="ij")
+    nyz, nyy, nyx = np.meshgrid(nqz, nqy, nqx, indexing="ij")
+    bx = np.where(nyx, 0, Bh[0]); by = np.where(nyy, 0, Bh[1]); bz = np.where(nyz, 0, Bh[2])
+    tnx, tny, tnz = np.tan(thx), np.tan(thy), np.tan(thz)
+    t2 = tnx * tnx + tny * tny + tnz * tnz
+    dot = np.where(t2 > 0, (tnx * bx + tny * by + tnz * bz) / np.where(t2 > 0, t2, 1.0), 0)
+    bx = bx - tnx * dot; by = by - tny * dot; bz = bz - tnz * dot
+    Fx = bx * np.exp(-1j * thx) / np.cos(thx)
+    Fy = by * np.exp(-1j * thy) / np.cos(thy)
+    Fz = bz * np.exp(-1j * thz) / np.cos(thz)
+    faces = [np.fft.irfftn(F, s=(nz, ny, nx)).ravel() for F in (Fx, Fy, Fz)]
+    dev = torch.device("cuda", s.device)
+    s.ct.slot(18).zero_(); s.ct.slot(19).zero_(); s.ct.slot(20).zero_()
+    for d in range(3):
+        s.ct.slot(d).copy_(torch.from_numpy(faces[d].astype(np.float32)).to(dev))
+    # cell B <- face average, E keeps p, psi <- 0 (ct.jl:205-219), done on the host in FP32
+    f32 = [f.astype(np.float32).reshape(nz, ny, nx) for f in faces]
+    hb = fields_to_host(s)
+    bxc = (np.float32(0.5) * (f32[0] + np.roll(f32[0], -1, axis=2))).ravel()
+    byc = (np.float32(0.5) * (f32[1] + np.roll(f32[1], -1, axis=1))).ravel()
+    bzc = (np.float32(0.5) * (f32[2] + np.roll(f32[2], -1, axis=0))).ravel()
+    ox, oy, oz = hb[5], hb[6], hb[7]
+    hb[4] = hb[4] + np.float32(0.5) * ((bxc * bxc + byc * byc + bzc * bzc) - (ox * ox + oy * oy + oz * oz))
+    hb[5], hb[6], hb[7], hb[8] = bxc, byc, bzc, 0
+    set_fields(s, hb)
+    Bnew = [hb[5 + d].astype(np.float64) for d in range(3)]
+    num = sum(((Bnew[d] - Bold[d].ravel()) ** 2).sum() for d in range(3))
+    den = sum((Bold[d] ** 2).sum() for d in range(3))
+    enew = sum((Bnew[d] ** 2).sum() for d in range(3))
+    brms = np.sqrt(enew / s.nc)
+    return {"cell_b_rel_l2_change": float(np.sqrt(num / den)) if den > 0 else 0.0,
+            "magnetic_energy_ratio": float(enew / den) if den > 0 else 1.0,
+            "max_divb_face_dx_over_brms": float(max_divb_face(s) * s.dx / brms) if brms > 0 else 0.0}
+
+
+# ---- batched boxes ---------------------------------------------------------------------
+class Batch:
+    """Many independent periodic boxes advanced together (pmfmhd_batch_*)."""
+
+    def __init__(self, states, cfl=0.2, glm_ch_fac=1.0, glm_cr=GLM_CR, device=None):
+        self.states = list(states)
+        boxes = (Box * len(self.states))()
+        for b, s in zip(boxes, self.states):
+            b.grid = s.grid
+            b.U = _P9(*[t.data_ptr() for t in s.U])
+            b.scratch = _P9(*[t.data_ptr() for t in s.scratch])
+            b.ct_packed = s.ct.packed.data_ptr() if s.ct is not None else None
+            b.resid = _P7(*([t.data_ptr() for t in s.resid] if s.resid is not None else [None] * 7))
+            b.mhd_solver = 1 if s.ct is not None else 0
+            b.cfl, b.glm_ch_fac, b.glm_cr = cfl, glm_ch_fac, glm_cr
+        self._boxes = boxes
+        self.device = self.states[0].device if device is None else device
+        h = _VP()
+        _check(lib().pmfmhd_batch_create(context(self.device), boxes, len(self.states), ctypes.byref(h)),
+               "batch_create")
+        self.handle = h
+
+    def step(self, nsteps=1):
+        _check(lib().pmfmhd_batch_step(self.handle, int(nsteps), _stream()), "batch_step")
+
+    def query(self):
+        n = len(self.states)
+        t = (ctypes.c_double * n)()
+        par = (ctypes.c_int32 * n)()
+        dt = (ctypes.c_float * n)()
+        _check(lib().pmfmhd_batch_query(self.handle, t, par, dt), "batch_query")
+        return np.array(t), np.array(par), np.array(dt)
+
+    def current_fields(self, i):
+        """Host copy of box i's current state (U or scratch, by the parity from query)."""
+        _, par, _ = self.query()
+        s = self.states[i]
+        src = s.scratch if par[i] else s.U
+        return torch.stack(src).cpu().numpy()
+
+    def close(self):
+        if self.handle:
+            lib().pmfmhd_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,245 @@
+"""Parity of the CUDA library (through its C ABI) with the CPU oracle on the reference's
+own test cases. Gates follow test/test_backends.jl:65-121 (per field
+max|cand-ref| <= 2e-6 + 5e-5*max|ref|, positive density, mass drift < 3e-6) and
+test/inherited/test_ct.jl for constrained transport."""
+import numpy as np
+import pytest
+import torch
+
+import fk_port
+import oracle
+import pmfmhd
+import problems
+from mhd_cases import KNOWN, alfven_L1, within_parity
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_state(U, dims, **kw):
+    s = pmfmhd.allocate_state(dims, 1.0 / max(dims) if "dx" not in kw else kw.pop("dx"), **kw)
+    pmfmhd.set_fields(s, U)
+    return s
+
+
+def oracle_state(U, dims, **kw):
+    kw = dict(kw)
+    dx = kw.pop("dx", 1.0 / max(dims))
+    s = oracle.OracleState(dims, dx, **kw)
+    s.U[:] = U
+    return s
+
+
+@pytest.mark.parametrize("recon", ["plm", "ppm", "plm_minmod"])
+@pytest.mark.parametrize("riemann", ["hlld", "hll", "llf"])
+def test_smooth_glm_matches_oracle(recon, riemann):
+    """test_backends.jl:76-121: N=16 smooth field, 3 steps at cfl 0.08."""
+    n = 16
+    U = problems.smooth_fields(n)
+    cpu = oracle_state(U, (n, n, n), recon=recon, riemann=riemann)
+    dev = gpu_state(U, (n, n, n), recon=recon, riemann=riemann)
+    dt, speed = cpu.compute_dt(0.08)
+    for _ in range(3):
+        cpu.step(dt, ch=speed)
+        pmfmhd.step(dev, float(dt), ch=float(speed))
+    host = pmfmhd.fields_to_host(dev)
+    assert not within_parity(cpu.U, host)
+    assert host[0].min() > 0
+    m0 = U[0].astype(np.float64).sum()
+    assert abs(host[0].astype(np.float64).sum() / m0 - 1) < KNOWN["parity"]["mass_drift"]
+    assert np.abs(host[1] - U[1]).max() > 1e-7  # the state evolved
+
+
+@pytest.mark.parametrize("dims", [(37, 11, 5), (64, 8, 3), (30, 9, 17), (7, 40, 6)])
+def test_ragged_grids_match_oracle(dims):
+    """Extents that are not multiples of the CTA tile (partial tiles, short z chunks)."""
+    U = problems.turb_field(dims, 1.0 / max(dims))
+    cpu = oracle_state(U, dims)
+    dev = gpu_state(U, dims)
+    dt, speed = cpu.compute_dt(0.2)
+    for _ in range(4):
+        cpu.step(dt, ch=speed)
+        pmfmhd.step(dev, float(dt), ch=float(speed))
+    assert not within_parity(cpu.U, pmfmhd.fields_to_host(dev))
+
+
+@pytest.mark.parametrize("bcs", [("outflow", "periodic", "periodic"), ("reflecting", "outflow", "reflecting"),
+                                 ("periodic", "reflecting", "outflow")])
+def test_boundary_conditions_match_oracle(bcs):
+    dims = (40, 12, 10)
+    U = problems.turb_field(dims, 1.0 / 40)
+    cpu = oracle_state(U, dims, bcs=bcs)
+    dev = gpu_state(U, dims, bcs=bcs)
+    dt, speed = cpu.compute_dt(0.2)
+    for _ in range(4):
+        cpu.step(dt, ch=speed)
+        pmfmhd.step(dev, float(dt), ch=float(speed))
+    assert not within_parity(cpu.U, pmfmhd.fields_to_host(dev))
+
+
+def test_compensated_matches_oracle():
+    n = 24
+    U = problems.smooth_fields(n)
+    cpu = oracle_state(U, (n, n, n), compensated=True)
+    dev = gpu_state(U, (n, n, n), compensated=True)
+    dt, speed = cpu.compute_dt(0.2)
+    for _ in range(5):
+        cpu.step(dt, ch=speed)
+        pmfmhd.step(dev, float(dt), ch=float(speed))
+    assert not within_parity(cpu.U, pmfmhd.fields_to_host(dev))
+    res = torch.stack(dev.resid).cpu().numpy()
+    assert np.abs(res).max() > 0  # remainders are being carried
+    assert np.abs(res - cpu.resid).max() <= 1e-6 * np.abs(cpu.U[1:8]).max() + 1e-9
+
+
+def test_alfven_evolve_matches_known_answer():
+    """The reference's convergence case end to end on the GPU (evolve with on-device CFL)."""
+    ref = KNOWN["alfven"]["plm_64"]
+
+    def make(dims, dx, recon):
+        s = pmfmhd.allocate_state(dims, dx, recon=recon)
+        return pmfmhd.set_fields(s, problems.alfven_wave(dims, dx, amp=0.1, B0=1.0, p0=0.1))
+    L1, n, _, drift = alfven_L1(make, pmfmhd.fields_to_host, pmfmhd.conserved_totals,
+                                lambda s, tf, cfl, cr: pmfmhd.evolve(s, tf, cfl=cfl, glm_cr=cr), 64)
+    assert n == ref["steps"]
+    assert abs(L1 / ref["L1"] - 1) < 0.02
+    assert drift["mass"] < 1e-4 and drift["energy"] < 1e-4
+
+
+def test_brio_wu_outflow_matches_oracle():
+    dims = (256, 4, 4)
+    U = problems.brio_wu(dims, gamma=2.0)
+    kw = dict(dx=1 / 256, gamma=2.0, bcs=("outflow", "periodic", "periodic"))
+    cpu = oracle_state(U, dims, **kw)
+    dev = gpu_state(U, dims, **kw)
+    t0, n0 = cpu.evolve(0.1, cfl=0.4)
+    t1, n1 = pmfmhd.evolve(dev, 0.1, cfl=0.4)
+    assert n0 == n1
+    rho = pmfmhd.fields_to_host(dev)[0][:256]
+    assert abs(rho.min() - KNOWN["brio_wu"]["rho_min"]) < 2e-3
+    assert np.abs(rho - cpu.U[0][:256]).max() < 1e-3
+
+
+def test_wavespeed_and_diagnostics_match_oracle():
+    dims = (48, 20, 12)
+    U = problems.turb_field(dims, 1 / 48)
+    cpu = oracle_state(U, dims, bcs=("periodic", "reflecting", "outflow"))
+    dev = gpu_state(U, dims, bcs=("periodic", "reflecting", "outflow"))
+    assert abs(pmfmhd.max_wavespeed(dev) / float(cpu.max_wavespeed()) - 1) < 1e-6
+    dt, sm = pmfmhd.compute_dt(dev, 0.3)
+    dt0, sm0 = cpu.compute_dt(0.3)
+    assert abs(dt / float(dt0) - 1) < 1e-6
+    assert abs(pmfmhd.max_divb(dev) - cpu.max_divb()) <= 1e-5 * max(1.0, cpu.max_divb())
+    tg, tc = pmfmhd.conserved_totals(dev), cpu.conserved_totals()
+    for k in tg:
+        assert abs(tg[k] - tc[k]) <= 1e-9 * max(1.0, abs(tc[k])), k
+
+
+def test_fused_wavespeed_equals_standalone():
+    n = 32
+    dev = gpu_state(problems.turb_field((n, n, n), 1 / n), (n, n, n))
+    dt, sm = pmfmhd.compute_dt(dev, 0.2)
+    pmfmhd.step(dev, dt, ch=sm)
+    assert pmfmhd.last_wavespeed(dev) == pmfmhd.max_wavespeed(dev)
+
+
+def test_graph_replay_equals_individual_steps():
+    n = 32
+    U = problems.turb_field((n, n, n), 1 / n)
+    a = gpu_state(U, (n, n, n))
+    b = gpu_state(U, (n, n, n))
+    dt, sm = pmfmhd.compute_dt(a, 0.2)
+    decay = float(np.exp(np.float32(np.float32(-0.18 * sm) * np.float32(dt)) / np.float32(a.dx)))
+    for _ in range(5):
+        pmfmhd.step_cube(a, dt, sm, decay)
+    pmfmhd.run_glm(b, 5, dt, sm, decay)
+    pmfmhd.run_glm(b, 5, dt, sm, decay)  # cached graph replay
+    for _ in range(5):
+        pmfmhd.step_cube(a, dt, sm, decay)
+    assert np.array_equal(pmfmhd.fields_to_host(a), pmfmhd.fields_to_host(b))
+
+
+def test_tile_shape_does_not_change_results():
+    """Every tile shape runs the same per-face arithmetic: results are bit-identical."""
+    n = 64
+    U = problems.turb_field((n, n, n), 1 / n)
+    a = gpu_state(U, (n, n, n))
+    b = gpu_state(U, (n, n, n))
+    dt, sm = pmfmhd.compute_dt(a, 0.2)
+    pmfmhd.step(a, dt, ch=sm)
+    pmfmhd.autotune(b)
+    pmfmhd.step(b, dt, ch=sm)
+    assert np.array_equal(pmfmhd.fields_to_host(a), pmfmhd.fields_to_host(b))
+
+
+def test_periodic_shift_invariance():
+    """step(shift(U)) == shift(step(U)) bit for bit: tile boundaries leave no trace."""
+    n = 48
+    U = problems.turb_field((n, n, n), 1 / n) * np.float32(1.0)
+    U[0] += np.float32(0.05) * np.sin(np.arange(U.shape[1]) * 0.37).astype(np.float32)
+    sh = lambda X: np.roll(X.reshape(9, n, n, n), (5, 11, 17), axis=(1, 2, 3)).reshape(9, -1)
+    a = gpu_state(U, (n, n, n))
+    b = gpu_state(sh(U), (n, n, n))
+    dt, sm = pmfmhd.compute_dt(a, 0.2)
+    pmfmhd.step(a, dt, ch=sm)
+    pmfmhd.step(b, dt, ch=sm)
+    assert np.array_equal(sh(pmfmhd.fields_to_host(a)), pmfmhd.fields_to_host(b))
+
+
+# ---- constrained transport -----------------------------------------------------------
+@pytest.mark.parametrize("riemann", ["hlld", "hll"])
+def test_ct_matches_oracle(riemann):
+    """test_backends.jl:353-405: CT on the smooth field, faces from the cells."""
+    n = 16
+    U = problems.smooth_fields(n)
+    dev = gpu_state(U, (n, n, n), riemann=riemann, mhd_solver="ct")
+    info = pmfmhd.ct_faces_from_cells(dev)
+    assert info["max_divb_face_dx_over_brms"] < 1e-5
+    cpu = oracle_state(pmfmhd.fields_to_host(dev), (n, n, n), riemann=riemann, mhd_solver="ct")
+    cpu.faces[:] = dev.ct.packed[: 3 * n ** 3].cpu().numpy().reshape(3, -1)
+    dt, _ = cpu.compute_dt(0.08)
+    for _ in range(3):
+        cpu.step(dt)
+        pmfmhd.step(dev, float(dt), integrator="ref")
+    host = pmfmhd.fields_to_host(dev)
+    assert not within_parity(cpu.U, host)
+    faces = dev.ct.packed[: 3 * n ** 3].cpu().numpy().reshape(3, -1)
+    for d in range(3):
+        assert np.abs(faces[d] - cpu.faces[d]).max() <= 2e-6 + 5e-5 * np.abs(cpu.faces[d]).max()
+    brms = np.sqrt((host[5:8].astype(np.float64) ** 2).sum() / n ** 3)
+    assert pmfmhd.max_divb_face(dev) * dev.dx / brms < 1e-5
+    assert np.all(host[8] == 0)
+
+
+def test_ct_from_potential_matches_oracle():
+    N = 24
+    g = 5 / 3
+    U = fk_port.ct_test_hydro(N, g).astype(np.float32)
+    A = fk_port.ct_test_potential(N).astype(np.float32)
+    dev = gpu_state(U, (N, N, N), mhd_solver="ct", riemann="hlld")
+    pmfmhd.ct_faces_from_potential(dev, A[0], A[1], A[2])
+    cpu = oracle_state(U, (N, N, N), mhd_solver="ct", riemann="hlld")
+    cpu.ct_faces_from_potential(A)
+    assert not within_parity(cpu.U, pmfmhd.fields_to_host(dev))
+    dt, _ = cpu.compute_dt(0.3)
+    for _ in range(6):
+        cpu.step(dt)
+        pmfmhd.step(dev, float(dt), integrator="ref")
+    assert not within_parity(cpu.U, pmfmhd.fields_to_host(dev))
+    assert pmfmhd.max_divb_face(dev) * dev.dx < 1e-6
+
+
+def test_ct_compensated_faces_match_oracle():
+    N = 16
+    U = fk_port.ct_test_hydro(N, 5 / 3).astype(np.float32)
+    A = fk_port.ct_test_potential(N).astype(np.float32)
+    dev = gpu_state(U, (N, N, N), mhd_solver="ct", compensated=True)
+    pmfmhd.ct_faces_from_potential(dev, A[0], A[1], A[2])
+    cpu = oracle_state(U, (N, N, N), mhd_solver="ct", compensated=True)
+    cpu.ct_faces_from_potential(A)
+    dt, _ = cpu.compute_dt(0.3)
+    for _ in range(4):
+        cpu.step(dt)
+        pmfmhd.step_ref(dev, float(dt), 0.0, 1.0, compensate_faces=True)
+    assert not within_parity(cpu.U, pmfmhd.fields_to_host(dev))
+    rb = torch.stack([dev.ct.rbx, dev.ct.rby, dev.ct.rbz]).cpu().numpy()
+    assert np.abs(rb).max() > 0
