@@ -239,6 +239,7 @@ inline void bcidx(int i, int n, int code, int& ii, int& flip) {
   if (i < 0) { ii = -1 - i; flip = -1; }
   else if (i >= n) { ii = 2 * n - 1 - i; flip = -1; }
   else ii = i;
+  ii = ii < 0 ? 0 : (ii >= n ? n - 1 : ii);  // axis shorter than the stencil
 }
 inline long lin(const Grid& g, int i, int j, int k) { return ((long)k * g.ny + j) * g.nx + i; }
 inline long per(const Grid& g, int i, int j, int k) {

@@ -150,7 +150,7 @@ class OracleState:
     def conserved_totals(self):
         out = np.zeros(8)
         self._f("totals")(ctypes.byref(self.p), _ptr(self.U), _ptr(out))
-        dV = float(self.dx) ** 3
+        dV = float(self.dx * self.dx * self.dx)  # s.dx^3 in the state's precision (diagnostics.jl:45)
         keys = ("mass", "momx", "momy", "momz", "energy", "Bx", "By", "Bz")
         return {k: v * dV for k, v in zip(keys, out)}
 

@@ -359,9 +359,11 @@ __device__ __forceinline__ int bc_index(int i, int n, int code, float* flip) {
     return r < 0 ? r + n : r;
   }
   if (code == BC_OUTFLOW) return i < 0 ? 0 : (i >= n ? n - 1 : i);
-  if (i < 0) { *flip = -1.0f; return -1 - i; }
-  if (i >= n) { *flip = -1.0f; return 2 * n - 1 - i; }
-  return i;
+  int r = i;
+  if (i < 0) { *flip = -1.0f; r = -1 - i; }
+  else if (i >= n) { *flip = -1.0f; r = 2 * n - 1 - i; }
+  // an axis shorter than the 2-cell stencil mirrors past its far end: clamp
+  return r < 0 ? 0 : (r >= n ? n - 1 : r);
 }
 
 __device__ __forceinline__ float warp_max(float v) {
