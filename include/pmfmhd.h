@@ -119,6 +119,19 @@ int pmfmhd_conserved_totals(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* 
                             void* stream);
 
 /*
+ * The same FP64 totals without a context and without allocating anything. No counterpart
+ * in the reference. For callers that cannot call cudaMalloc (a host that owns the device
+ * memory pool, a plugin inside another application, code that must not allocate between
+ * steps): the scratch is a 4 MiB file-scope __device__ array of this library, held by every
+ * GPU that loads it until exit. At most 2^24 cells (256^3); larger grids return
+ * PMFMHD_ESHAPE. One partial sum per 256-cell block in a fixed order, so the result does not
+ * depend on the SM count. Calls share the array: calls that overlap on the GPU race and
+ * must be serialised. The first call on a device looks up the array's address; make it
+ * before any stream capture. Blocking.
+ */
+int pmfmhd_conserved_totals_noalloc(const pmfmhd_grid* g, const float* const U[9], double out[8], void* stream);
+
+/*
  * CT initialisation from an EDGE-centred vector potential A (3 device arrays, Ax at
  * (i,j-1/2,k-1/2), Ay at (i-1/2,j,k-1/2), Az at (i-1/2,j-1/2,k)): faces = discrete curl,
  * cell B = face average, E adjusted to keep the thermal pressure, psi = 0, face remainders

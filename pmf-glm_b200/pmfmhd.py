@@ -69,6 +69,7 @@ SIGNATURES = {
     "pmfmhd_max_divb": ([_VP, _GP, _P9, ctypes.POINTER(ctypes.c_double), _VP], ctypes.c_int),
     "pmfmhd_max_divb_face": ([_VP, _GP, _VP, ctypes.POINTER(ctypes.c_double), _VP], ctypes.c_int),
     "pmfmhd_conserved_totals": ([_VP, _GP, _P9, ctypes.c_double * 8, _VP], ctypes.c_int),
+    "pmfmhd_conserved_totals_noalloc": ([_GP, _P9, ctypes.c_double * 8, _VP], ctypes.c_int),
     "pmfmhd_ct_faces_from_potential": ([_VP, _GP, _P3, _P9, _VP, _VP], ctypes.c_int),
     "pmfmhd_run_glm": ([_VP, _GP, _P9, _P9, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, _VP, _VP],
                        ctypes.c_int),
