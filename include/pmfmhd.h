@@ -180,6 +180,12 @@ int pmfmhd_batch_destroy(pmfmhd_batch* b);
 int pmfmhd_autotune(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], int mhd_solver,
                     int compensated, void* stream);
 
+/* Pin (or query) the tile used for this grid/solver/mode on this context: `rows` owned rows
+ * per CTA (an instantiated height: 4, 8 or 14) and `planes` z-planes per CTA chunk. */
+int pmfmhd_set_tile(pmfmhd_ctx* ctx, const pmfmhd_grid* g, int mhd_solver, int compensated, int rows, int planes);
+int pmfmhd_get_tile(pmfmhd_ctx* ctx, const pmfmhd_grid* g, int mhd_solver, int compensated, int* rows,
+                    int* planes);
+
 #ifdef __cplusplus
 }
 #endif

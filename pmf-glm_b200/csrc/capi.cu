@@ -110,14 +110,12 @@ int aux_blocks(const pmfmhd_ctx* c, long long nc) {
   return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
 }
 
-Tune default_tune(const pmfmhd_ctx* c, const pmfmhd_grid* g) {
+// Tile height and the minimum number of planes per CTA (the launch gives every CTA an
+// equal share of the (column, plane) space, but never less than `tz` planes).
+Tune default_tune(const pmfmhd_ctx*, const pmfmhd_grid* g) {
   Tune t;
-  t.ty = g->ny >= 8 ? 8 : 4;
-  const long long cols = (long long)((g->nx + TILE_X - 1) / TILE_X) * ((g->ny + t.ty - 1) / t.ty);
-  // enough CTAs for about two resident waves, but chunks of at least 16 planes
-  long long want = (2LL * c->sms + cols - 1) / cols;
-  int nzc = (int)std::max<long long>(1, std::min<long long>(want, (g->nz + 15) / 16));
-  t.tz = (g->nz + nzc - 1) / nzc;
+  t.ty = g->ny >= 14 ? 14 : (g->ny >= 8 ? 8 : 4);
+  t.tz = 16;
   return t;
 }
 
@@ -128,19 +126,37 @@ Tune tune_for(pmfmhd_ctx* c, const pmfmhd_grid* g, bool ct, bool comp) {
   return default_tune(c, g);
 }
 
-int launch_step(const pmfmhd_grid* g, StepArgs& a, Tune t, bool ct, bool comp, cudaStream_t s) {
+// Resident CTAs per SM of a step kernel (cached per kernel).
+int occupancy_of(const StepKernelInfo& k) {
+  static std::mutex mu;
+  static std::map<const void*, int> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find((const void*)k.fn);
+  if (it != cache.end()) return it->second;
+  int occ = 1;
+  if (cudaFuncSetAttribute((const void*)k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_bytes) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k.fn, k.threads, k.smem_bytes) != cudaSuccess ||
+      occ < 1)
+    occ = 1;
+  cache[(const void*)k.fn] = occ;
+  return occ;
+}
+
+int launch_step(const pmfmhd_ctx* c, const pmfmhd_grid* g, StepArgs& a, Tune t, bool ct, bool comp,
+                cudaStream_t s) {
   StepKernelInfo k = step_kernel_info(t.ty, g->recon, g->riemann, ct, comp);
   if (k.fn == nullptr) return PMFMHD_EUNSUPPORTED;
-  PMF_CK(cudaFuncSetAttribute((const void*)k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_bytes));
+  const int occ = occupancy_of(k);
   a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
   for (int d = 0; d < 3; ++d) a.bc[d] = g->bc[d];
   a.ntx = (g->nx + TILE_X - 1) / TILE_X;
   a.nty = (g->ny + t.ty - 1) / t.ty;
-  a.tz = t.tz;
-  a.nzc = (g->nz + t.tz - 1) / t.tz;
   a.P = phys_of(g);
-  const long long blocks = (long long)a.ntx * a.nty * a.nzc;
-  if (blocks >= (1LL << 31)) return PMFMHD_ESHAPE;
+  const long long Q = (long long)a.ntx * a.nty * g->nz;
+  const long long slots = (long long)c->sms * occ;
+  const long long by_work = std::max<long long>(1, (Q + t.tz - 1) / std::max(1, t.tz));
+  const long long blocks = std::min(slots, by_work);
   void* args[] = {(void*)&a};
   PMF_CK(cudaLaunchKernel((const void*)k.fn, dim3((unsigned)blocks), dim3(k.threads), args, k.smem_bytes, s));
   return PMFMHD_OK;
@@ -163,7 +179,7 @@ int enqueue_glm(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], fl
   const float dtdx = dt / g->dx;  // T(dt)/s.dx (integrator_ref.jl:211)
   fill_glm_args(a, U, Un, resid, comp, dtdx, ch, decay, c->d_smax);
   PMF_CK(cudaMemsetAsync(c->d_smax, 0, sizeof(unsigned int), s));
-  return launch_step(g, a, tune_for(c, g, false, comp), false, comp, s);
+  return launch_step(c, g, a, tune_for(c, g, false, comp), false, comp, s);
 }
 
 int enqueue_ct(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Un[9], float* ct, float dt,
@@ -174,7 +190,7 @@ int enqueue_ct(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], flo
   fill_glm_args(a, U, Un, resid, comp, dtdx, 0.0f, 1.0f, nullptr);
   for (int d = 0; d < 3; ++d) a.face[d] = ct + (size_t)(CT_BXF + d) * nc;
   for (int k = 0; k < CT_NWORK; ++k) a.work[k] = ct + (size_t)(CT_MFX + k) * nc;
-  int rc = launch_step(g, a, tune_for(c, g, true, comp), true, comp, s);
+  int rc = launch_step(c, g, a, tune_for(c, g, true, comp), true, comp, s);
   if (rc != PMFMHD_OK) return rc;
   const int nb = aux_blocks(c, nc);
   ct_emf_kernel<<<nb, AUX_THREADS, 0, s>>>(ct, g->nx, g->ny, g->nz);
@@ -425,7 +441,7 @@ int pmfmhd_run_glm(pmfmhd_ctx* c, const pmfmhd_grid* g, float* const U[9], float
     StepArgs a;
     fill_glm_args(a, src, dst, resid, comp, dtdx, ch, decay, c->d_smax);
     cudaMemsetAsync(c->d_smax, 0, sizeof(unsigned int), c->cap);
-    int lrc = launch_step(g, a, t, false, comp, c->cap);
+    int lrc = launch_step(c, g, a, t, false, comp, c->cap);
     if (lrc != PMFMHD_OK) {
       cudaGraph_t dead;
       cudaStreamEndCapture(c->cap, &dead);
@@ -483,11 +499,10 @@ int pmfmhd_autotune(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9]
   if (ct) cudaMemsetAsync(ctp, 0, (size_t)CT_NSLOT * nc * sizeof(float), s);
   Tune best = default_tune(c, g);
   float best_ms = 1e30f;
-  std::vector<int> tzs = {g->nz, 256, 128, 64, 32, 16};
+  std::vector<int> tzs = {8, 32};
   for (int ty : kTileRows) {
     if (ty > 4 && g->ny < ty) continue;
     for (int tz : tzs) {
-      if (tz > g->nz || tz < 1) continue;
       Tune t{ty, tz};
       float ms_sum = 0.0f;
       for (int rep = 0; rep < 4 && result == PMFMHD_OK; ++rep) {
@@ -499,7 +514,7 @@ int pmfmhd_autotune(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9]
           a.smax_bits = nullptr;
         }
         cudaEventRecord(e0, s);
-        int lrc = launch_step(g, a, t, ct, comp, s);
+        int lrc = launch_step(c, g, a, t, ct, comp, s);
         cudaEventRecord(e1, s);
         if (lrc != PMFMHD_OK) { result = lrc; break; }
         if (cudaEventSynchronize(e1) != cudaSuccess) { result = PMFMHD_ECUDA; break; }
@@ -520,6 +535,29 @@ int pmfmhd_autotune(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9]
     c->tune[TuneKey{g->nx, g->ny, g->nz, ct, comp, g->recon, g->riemann}] = best;
   }
   return result;
+}
+
+int pmfmhd_set_tile(pmfmhd_ctx* c, const pmfmhd_grid* g, int mhd_solver, int compensated, int rows, int planes) {
+  if (c == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  bool known = false;
+  for (int ty : kTileRows) known |= ty == rows;
+  if (!known || planes < 1) return PMFMHD_EINVAL;
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->tune[TuneKey{g->nx, g->ny, g->nz, mhd_solver == 1, compensated != 0, g->recon, g->riemann}] =
+      Tune{rows, std::min(planes, g->nz)};
+  return PMFMHD_OK;
+}
+
+int pmfmhd_get_tile(pmfmhd_ctx* c, const pmfmhd_grid* g, int mhd_solver, int compensated, int* rows, int* planes) {
+  if (c == nullptr || rows == nullptr || planes == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  const Tune t = tune_for(c, g, mhd_solver == 1, compensated != 0);
+  *rows = t.ty;
+  *planes = t.tz;
+  return PMFMHD_OK;
 }
 
 }  // extern "C"

@@ -13,8 +13,8 @@ struct StepKernelInfo {
 };
 
 // Rows per CTA that are instantiated (tile candidates for the autotuner).
-constexpr int kTileRows[] = {4, 8};
-constexpr int kNumTileRows = 2;
+constexpr int kTileRows[] = {4, 8, 14};
+constexpr int kNumTileRows = 3;
 
 StepKernelInfo step_kernel_info(int ty, int recon, int rsol, bool ct, bool comp);
 }  // namespace pmf

@@ -1,0 +1,17 @@
+// Host-side dispatch over the instantiated tile heights.
+#include "dispatch.h"
+
+namespace pmf {
+StepKernelInfo step_kernel_info_ty4(int recon, int rsol, bool ct, bool comp);
+StepKernelInfo step_kernel_info_ty8(int recon, int rsol, bool ct, bool comp);
+StepKernelInfo step_kernel_info_ty14(int recon, int rsol, bool ct, bool comp);
+
+StepKernelInfo step_kernel_info(int ty, int recon, int rsol, bool ct, bool comp) {
+  switch (ty) {
+    case 4: return step_kernel_info_ty4(recon, rsol, ct, comp);
+    case 8: return step_kernel_info_ty8(recon, rsol, ct, comp);
+    case 14: return step_kernel_info_ty14(recon, rsol, ct, comp);
+  }
+  return StepKernelInfo{nullptr, 0, 0};
+}
+}  // namespace pmf

@@ -41,7 +41,7 @@ struct StepArgs {
   float* work[CT_NWORK];    // CT: mfx mfy mfz fxby fxbz fybx fybz fzbx fzby ecx ecy ecz
   int nx, ny, nz;
   int bc[3];
-  int ntx, nty, nzc, tz;    // tiles along x, y; z chunks and planes per chunk
+  int ntx, nty;             // column tiles along x and y
   float dtdx, ch, decay;
   Phys P;
   unsigned int* smax_bits;  // fused CFL reduction target (bits of a non-negative float), or null
@@ -66,12 +66,14 @@ __device__ __forceinline__ void cp_async4(float* smem_dst, const float* gsrc) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// One column segment: planes [z0, z1) of column tile (tx, ty) of the box described by `a`.
+// Every thread of the CTA calls it; `smax` accumulates the new state's max signal speed.
 template <int TY, int RECON, int RSOL, bool CT, bool COMP>
-__global__ void __launch_bounds__(32 * (TY + 2), 1) mhd_step_kernel(const StepArgs a) {
+__device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, int z0, int z1, float* smem,
+                                             float& smax) {
   using S = StepSmem<TY>;
   constexpr int NT = 32 * (TY + 2);
   constexpr int PP = S::PP;
-  extern __shared__ float smem[];
   float* stage = smem;
   float* prim = smem + S::STAGE;
   float* ybuf = prim + S::PRIM;
@@ -79,11 +81,7 @@ __global__ void __launch_bounds__(32 * (TY + 2), 1) mhd_step_kernel(const StepAr
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5;
-  const int bid = blockIdx.x;
-  const int tx = bid % a.ntx, ty = (bid / a.ntx) % a.nty, zc = bid / (a.ntx * a.nty);
   const int x0 = tx * TILE_X, y0 = ty * TY;
-  const int z0 = zc * a.tz;
-  const int z1 = min(z0 + a.tz, a.nz);
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int nxy = nx * ny;
 
@@ -140,6 +138,7 @@ __global__ void __launch_bounds__(32 * (TY + 2), 1) mhd_step_kernel(const StepAr
   };
 
   // Prologue: primitives of planes z0-2 and z0-1, plane z0 in flight.
+  __syncthreads();
   issue_plane(z0 - 2);
   cp_async_wait_all();
   __syncthreads();
@@ -152,12 +151,58 @@ __global__ void __launch_bounds__(32 * (TY + 2), 1) mhd_step_kernel(const StepAr
   __syncthreads();
   issue_plane(z0);
 
-  // Per-column carries across planes.
+  // Per-column carries across planes (owned rows only).
   F9 zR;      // upper z-face state of plane p-1
   F9 Fzc;     // flux through the lower z-face of plane p-1
   F9 dUxy;    // (Fxl - Fxh) + (Fyl - Fyh) of plane p-1
-  float smax = 0.0f;
   const int r0 = w + 1, c0 = lane + 1;  // this thread's cell in the staged plane
+
+  // Conservative update of cell (x, y, pz) from its x/y divergence and its two z fluxes.
+  auto update_cell = [&](int pz, const F9& dxy, const F9& flo, const F9& fhi) {
+    const int c = pz * nxy + y * nx + x;
+    F9 u0;
+#pragma unroll
+    for (int f = 0; f < 9; ++f) u0[f] = __ldg(a.U[f] + c);
+    F9 un;
+    float d[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) d[i] = dtdx * (dxy[i] + (flo[i] - fhi[i]));
+    un[0] = u0[0] + d[0];
+    if constexpr (COMP) {
+#pragma unroll
+      for (int i = 1; i <= 4; ++i) {
+        float r = a.resid[i - 1][c];
+        un[i] = comp_add(u0[i], d[i], r);
+        a.resid[i - 1][c] = r;
+      }
+      if constexpr (!CT) {
+#pragma unroll
+        for (int i = 5; i <= 7; ++i) {
+          float r = a.resid[i - 1][c];
+          un[i] = comp_add(u0[i], d[i], r);
+          a.resid[i - 1][c] = r;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int i = 1; i <= 7; ++i) un[i] = u0[i] + d[i];
+    }
+    un[8] = CT ? 0.0f : (u0[8] + d[8]) * decay;
+#pragma unroll
+    for (int f = 0; f < 9; ++f) {
+      if (CT && f >= 5 && f <= 7) continue;  // cell B comes from the face average
+      a.Un[f][c] = un[f];
+    }
+    if (!CT && a.smax_bits != nullptr) smax = fmaxf(smax, cell_wavespeed(un, P));
+  };
+  // Staggered normal field of this thread's cell's lower face along axis D (CT).
+  auto face_bn = [&](int D, int pz) {
+    float f0;
+    const int ix = bc_index(x, nx, BC_PERIODIC, &f0);
+    const int iy = bc_index(y, ny, BC_PERIODIC, &f0);
+    const int kz = bc_index(pz, nz, BC_PERIODIC, &f0);
+    return __ldg(a.face[D] + kz * nxy + iy * nx + ix);
+  };
 
   for (int p = z0 - 1; p <= z1; ++p) {
     cp_async_wait_all();
@@ -165,6 +210,9 @@ __global__ void __launch_bounds__(32 * (TY + 2), 1) mhd_step_kernel(const StepAr
     convert_plane(p + 1, slot(p + 1));
     __syncthreads();
     if (p + 2 <= z1 + 1) issue_plane(p + 2);
+
+    // plane z0-1 only feeds the lower z-face of the chunk: the y-halo rows skip it
+    if (p == z0 - 1 && !row_own) continue;
 
     // ---- Hancock half step of this thread's cell in plane p ------------------------------
     const float* pm = slot(p - 1);
@@ -186,195 +234,181 @@ __global__ void __launch_bounds__(32 * (TY + 2), 1) mhd_step_kernel(const StepAr
       for (int i = 0; i < 9; ++i) uh[i] = u0[i] - h * acc[i];
       mh = cons2prim(uh, g, P.smallr, P.pfl);
     }
-    const int cell_p = (p >= 0 && p < nz && x < nx && y < ny) ? (p * nxy + y * nx + x) : 0;
-
+    const bool mid = p >= z0 && p < z1;  // an owned plane of this chunk
+    const int cell_p = (mid && x < nx && y < ny) ? (p * nxy + y * nx + x) : 0;
+    if constexpr (CT) {
+      // cell-centred reference EMF -v x B: v of the predicted state, B at the start of the
+      // step (integrator_ref.jl:133-138)
+      if (own && mid) {
+        a.work[9][cell_p] = mh[3] * m0[6] - mh[2] * m0[7];
+        a.work[10][cell_p] = mh[1] * m0[7] - mh[3] * m0[5];
+        a.work[11][cell_p] = mh[2] * m0[5] - mh[1] * m0[6];
+      }
+    }
     if (p == z0 - 1) {
       zR = face_hi<RECON>(mh, oz);
       continue;
     }
-
-    F9 Fz;
-    {
-      // z-face p-1/2: left = upper z state of plane p-1 (carried), right = lower z state of p
-      F9 L = zR, R = face_lo<RECON>(mh, oz);
-      if constexpr (CT) {
-        float zf;
-        const int kz = bc_index(p, nz, BC_PERIODIC, &zf);
-        float xf, yf;
-        const int ix = bc_index(x, nx, BC_PERIODIC, &xf), iy = bc_index(y, ny, BC_PERIODIC, &yf);
-        const float bn = __ldg(a.face[2] + kz * nxy + iy * nx + ix);
-        L[7] = bn; R[7] = bn;
-      }
-      Fz = riemann<2, RSOL, CT>(L, R, ch, P);
+    // y-halo row 0 and the owned rows publish their upper y state for the face above
+    if (mid && w <= TY) {
+      const F9 yR = face_hi<RECON>(mh, oy);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) ybuf[(w * 9 + i) * 32 + lane] = yR[i];
     }
-
-    if (p < z1) {
-      // ---- x-faces: lane l solves the face between cells l-1 and l ------------------------
-      F9 dx_flux;  // (Fxl - Fxh) for this cell
-      F9 Fx;
-      if (row_own) {
-        F9 L, R = face_lo<RECON>(mh, ox);
-        const F9 xR = face_hi<RECON>(mh, ox);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) L[i] = __shfl_up_sync(0xffffffffu, xR[i], 1);
+    if (row_own) {
+      // ---- z-face p-1/2: left = carried upper z state of p-1, right = lower z state of p --
+      F9 Fz;
+      {
+        F9 L = zR, R = face_lo<RECON>(mh, oz);
         if constexpr (CT) {
-          float f0;
-          const int ix = bc_index(x, nx, BC_PERIODIC, &f0);
-          const int iy = bc_index(y, ny, BC_PERIODIC, &f0);
-          const int kz = bc_index(p, nz, BC_PERIODIC, &f0);
-          const float bn = __ldg(a.face[0] + kz * nxy + iy * nx + ix);
-          L[5] = bn; R[5] = bn;
+          const float bn = face_bn(2, p);
+          L[7] = bn; R[7] = bn;
         }
-        Fx = riemann<0, RSOL, CT>(L, R, ch, P);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) dx_flux[i] = Fx[i] - __shfl_down_sync(0xffffffffu, Fx[i], 1);
+        Fz = riemann<2, RSOL, CT>(L, R, ch, P);
       }
-      // ---- y-faces: rows 0..TY publish their upper y state; rows 1..TY+1 solve ------------
-      if (w <= TY) {
-        const F9 yR = face_hi<RECON>(mh, oy);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) ybuf[(w * 9 + i) * 32 + lane] = yR[i];
-      }
-      __syncthreads();
-      F9 Fy;
-      if (w >= 1) {
-        F9 L, R = face_lo<RECON>(mh, oy);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) L[i] = ybuf[((w - 1) * 9 + i) * 32 + lane];
-        if constexpr (CT) {
-          float f0;
-          const int ix = bc_index(x, nx, BC_PERIODIC, &f0);
-          const int iy = bc_index(y, ny, BC_PERIODIC, &f0);
-          const int kz = bc_index(p, nz, BC_PERIODIC, &f0);
-          const float bn = __ldg(a.face[1] + kz * nxy + iy * nx + ix);
-          L[6] = bn; R[6] = bn;
-        }
-        Fy = riemann<1, RSOL, CT>(L, R, ch, P);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) fybuf[((w - 1) * 9 + i) * 32 + lane] = Fy[i];
-      }
-      __syncthreads();
-      F9 dUxy_p;
-      if (row_own) {
-#pragma unroll
-        for (int i = 0; i < 9; ++i) dUxy_p[i] = dx_flux[i] + (Fy[i] - fybuf[(w * 9 + i) * 32 + lane]);
-      }
+      zR = face_hi<RECON>(mh, oz);
       if constexpr (CT) {
-        // lower-face fluxes and the cell-centred reference EMF -v x B (v of the predicted
-        // state, B at the start of the step) for the edge EMFs (integrator_ref.jl:127-139)
-        if (own) {
-          a.work[0][cell_p] = Fx[0];
-          a.work[1][cell_p] = Fy[0];
+        if (own && mid) {
           a.work[2][cell_p] = Fz[0];
-          a.work[3][cell_p] = Fx[6];
-          a.work[4][cell_p] = Fx[7];
-          a.work[5][cell_p] = Fy[5];
-          a.work[6][cell_p] = Fy[7];
           a.work[7][cell_p] = Fz[5];
           a.work[8][cell_p] = Fz[6];
-          a.work[9][cell_p] = mh[3] * m0[6] - mh[2] * m0[7];
-          a.work[10][cell_p] = mh[1] * m0[7] - mh[3] * m0[5];
-          a.work[11][cell_p] = mh[2] * m0[5] - mh[1] * m0[6];
         }
       }
-      if (p > z0) {
-        // update plane p-1 with its carried x/y divergence and its two z fluxes
-        if (own) {
-          const int c = (p - 1) * nxy + y * nx + x;
-          F9 u0;
-#pragma unroll
-          for (int f = 0; f < 9; ++f) u0[f] = __ldg(a.U[f] + c);
-          F9 un;
-          float d[9];
-#pragma unroll
-          for (int i = 0; i < 9; ++i) d[i] = dtdx * (dUxy[i] + (Fzc[i] - Fz[i]));
-          un[0] = u0[0] + d[0];
-          if constexpr (COMP) {
-#pragma unroll
-            for (int i = 1; i <= 4; ++i) {
-              float r = a.resid[i - 1][c];
-              un[i] = comp_add(u0[i], d[i], r);
-              a.resid[i - 1][c] = r;
-            }
-            if constexpr (!CT) {
-#pragma unroll
-              for (int i = 5; i <= 7; ++i) {
-                float r = a.resid[i - 1][c];
-                un[i] = comp_add(u0[i], d[i], r);
-                a.resid[i - 1][c] = r;
-              }
-            }
-          } else {
-#pragma unroll
-            for (int i = 1; i <= 7; ++i) un[i] = u0[i] + d[i];
-          }
-          un[8] = CT ? 0.0f : (u0[8] + d[8]) * decay;
-#pragma unroll
-          for (int f = 0; f < 9; ++f) {
-            if (CT && f >= 5 && f <= 7) continue;  // cell B comes from the face average
-            a.Un[f][c] = un[f];
-          }
-          if (!CT && a.smax_bits != nullptr) smax = fmaxf(smax, cell_wavespeed(un, P));
-        }
-      }
-      if (row_own) dUxy = dUxy_p;
-      zR = face_hi<RECON>(mh, oz);
+      if (p > z0 && own) update_cell(p - 1, dUxy, Fzc, Fz);
       Fzc = Fz;
-    } else {
-      // p == z1: only the z-face z1-1/2 is needed; update the last owned plane.
-      if (own) {
-        const int c = (p - 1) * nxy + y * nx + x;
-        F9 u0;
+    }
+    if (!mid) continue;  // p == z1: only the last z-face and update were needed
+
+    // ---- x-faces: lane l solves the face between cells l-1 and l ------------------------
+    F9 dx_flux;  // (Fxl - Fxh) of this cell
+    if (row_own) {
+      F9 L, R = face_lo<RECON>(mh, ox);
+      const F9 xR = face_hi<RECON>(mh, ox);
 #pragma unroll
-        for (int f = 0; f < 9; ++f) u0[f] = __ldg(a.U[f] + c);
-        F9 un;
-        float d[9];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) d[i] = dtdx * (dUxy[i] + (Fzc[i] - Fz[i]));
-        un[0] = u0[0] + d[0];
-        if constexpr (COMP) {
-#pragma unroll
-          for (int i = 1; i <= 4; ++i) {
-            float r = a.resid[i - 1][c];
-            un[i] = comp_add(u0[i], d[i], r);
-            a.resid[i - 1][c] = r;
-          }
-          if constexpr (!CT) {
-#pragma unroll
-            for (int i = 5; i <= 7; ++i) {
-              float r = a.resid[i - 1][c];
-              un[i] = comp_add(u0[i], d[i], r);
-              a.resid[i - 1][c] = r;
-            }
-          }
-        } else {
-#pragma unroll
-          for (int i = 1; i <= 7; ++i) un[i] = u0[i] + d[i];
-        }
-        un[8] = CT ? 0.0f : (u0[8] + d[8]) * decay;
-#pragma unroll
-        for (int f = 0; f < 9; ++f) {
-          if (CT && f >= 5 && f <= 7) continue;
-          a.Un[f][c] = un[f];
-        }
-        if (!CT && a.smax_bits != nullptr) smax = fmaxf(smax, cell_wavespeed(un, P));
+      for (int i = 0; i < 9; ++i) L[i] = __shfl_up_sync(0xffffffffu, xR[i], 1);
+      if constexpr (CT) {
+        const float bn = face_bn(0, p);
+        L[5] = bn; R[5] = bn;
       }
+      const F9 Fx = riemann<0, RSOL, CT>(L, R, ch, P);
+      if constexpr (CT) {
+        if (own) {
+          a.work[0][cell_p] = Fx[0];
+          a.work[3][cell_p] = Fx[6];
+          a.work[4][cell_p] = Fx[7];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 9; ++i) dx_flux[i] = Fx[i] - __shfl_down_sync(0xffffffffu, Fx[i], 1);
+    }
+    __syncthreads();
+    // ---- y-faces: rows 1..TY+1 solve the face below them -------------------------------
+    F9 Fy;
+    if (w >= 1) {
+      F9 L, R = face_lo<RECON>(mh, oy);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) L[i] = ybuf[((w - 1) * 9 + i) * 32 + lane];
+      if constexpr (CT) {
+        const float bn = face_bn(1, p);
+        L[6] = bn; R[6] = bn;
+      }
+      Fy = riemann<1, RSOL, CT>(L, R, ch, P);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) fybuf[((w - 1) * 9 + i) * 32 + lane] = Fy[i];
+      if constexpr (CT) {
+        if (own) {
+          a.work[1][cell_p] = Fy[0];
+          a.work[5][cell_p] = Fy[5];
+          a.work[6][cell_p] = Fy[7];
+        }
+      }
+    }
+    __syncthreads();
+    if (row_own) {
+#pragma unroll
+      for (int i = 0; i < 9; ++i) dUxy[i] = dx_flux[i] + (Fy[i] - fybuf[(w * 9 + i) * 32 + lane]);
     }
   }
   cp_async_wait_all();
+}
 
-  if (!CT && a.smax_bits != nullptr) {
-    __shared__ float red[32];
-    __syncthreads();
-    float m = warp_max(smax);
-    if (lane == 0) red[w] = m;
-    __syncthreads();
-    if (w == 0) {
-      m = lane < (NT / 32) ? red[lane] : 0.0f;
-      m = warp_max(m);
-      if (lane == 0) atomicMax(a.smax_bits, __float_as_uint(m));
-    }
+// Block-wide max of v and one atomicMax into *bits (every thread of the CTA calls it).
+template <int NT>
+__device__ __forceinline__ void flush_smax(float v, unsigned int* bits) {
+  __shared__ float red[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  v = warp_max(v);
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = lane < NT / 32 ? red[lane] : 0.0f;
+    v = warp_max(v);
+    if (lane == 0) atomicMax(bits, __float_as_uint(v));
   }
+}
+
+// Planes [q0, q1) of a (column, plane) index space, q = column * nz + z, split into column
+// segments: CTA b of B takes [b*Q/B, (b+1)*Q/B), so every CTA does the same number of
+// planes (to within one) and the launch has no partial last wave.
+__device__ __forceinline__ void cta_range(long long Q, long long* q0, long long* q1) {
+  *q0 = Q * blockIdx.x / gridDim.x;
+  *q1 = Q * (blockIdx.x + 1) / gridDim.x;
+}
+
+// One box: a persistent launch of one CTA per resident slot.
+template <int TY, int RECON, int RSOL, bool CT, bool COMP>
+__global__ void __launch_bounds__(32 * (TY + 2), 1) mhd_step_kernel(const __grid_constant__ StepArgs a) {
+  extern __shared__ float smem[];
+  long long q, qe;
+  cta_range((long long)a.ntx * a.nty * a.nz, &q, &qe);
+  float smax = 0.0f;
+  while (q < qe) {
+    const int col = (int)(q / a.nz);
+    const int z0 = (int)(q - (long long)col * a.nz);
+    const int z1 = (int)min((long long)a.nz, z0 + (qe - q));
+    march_column<TY, RECON, RSOL, CT, COMP>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax);
+    q += z1 - z0;
+  }
+  if (!CT && a.smax_bits != nullptr) flush_smax<32 * (TY + 2)>(smax, a.smax_bits);
+}
+
+// Many boxes in one launch: box b owns global indices [q0_b, q0_{b+1}) of the concatenated
+// (column, plane) spaces; each CTA walks its equal share across box boundaries.
+struct BoxStep {
+  StepArgs a;     // per-box pointers, extents and parameters; dscal = that box's {dt/dx, ch, decay}
+  long long q0;   // first global (column, plane) index of this box
+};
+
+template <int TY, int RECON, int RSOL, bool CT, bool COMP>
+__global__ void __launch_bounds__(32 * (TY + 2), 1) mhd_batch_kernel(const BoxStep* __restrict__ boxes, int nbox,
+                                                                       long long Q) {
+  extern __shared__ float smem[];
+  long long q, qe;
+  cta_range(Q, &q, &qe);
+  if (q >= qe) return;
+  int b = 0, hi = nbox - 1;
+  while (b < hi) {  // last box with q0 <= q
+    const int mid = (b + hi + 1) >> 1;
+    if (boxes[mid].q0 <= q) b = mid;
+    else hi = mid - 1;
+  }
+  float smax = 0.0f;
+  while (q < qe) {
+    while (b + 1 < nbox && boxes[b + 1].q0 <= q) {
+      if (!CT && boxes[b].a.smax_bits != nullptr) flush_smax<32 * (TY + 2)>(smax, boxes[b].a.smax_bits);
+      smax = 0.0f;
+      ++b;
+    }
+    const StepArgs& a = boxes[b].a;
+    const long long local = q - boxes[b].q0;
+    const int col = (int)(local / a.nz);
+    const int z0 = (int)(local - (long long)col * a.nz);
+    const int z1 = (int)min((long long)a.nz, z0 + (qe - q));
+    march_column<TY, RECON, RSOL, CT, COMP>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax);
+    q += z1 - z0;
+  }
+  if (!CT && boxes[b].a.smax_bits != nullptr) flush_smax<32 * (TY + 2)>(smax, boxes[b].a.smax_bits);
 }
 
 }  // namespace pmf

@@ -1,0 +1,33 @@
+// Lookup of the step-kernel instantiations for one tile height (included by step_ty*.cu).
+#pragma once
+#include "dispatch.h"
+#include "step_kernel.cuh"
+
+namespace pmf {
+namespace detail {
+template <int TY, int RECON, int RSOL>
+StepKernel pick(bool ct, bool comp) {
+  if (ct) return comp ? mhd_step_kernel<TY, RECON, RSOL, true, true> : mhd_step_kernel<TY, RECON, RSOL, true, false>;
+  return comp ? mhd_step_kernel<TY, RECON, RSOL, false, true> : mhd_step_kernel<TY, RECON, RSOL, false, false>;
+}
+template <int TY, int RECON>
+StepKernel pick_rs(int rsol, bool ct, bool comp) {
+  switch (rsol) {
+    case RS_HLLD: return pick<TY, RECON, RS_HLLD>(ct, comp);
+    case RS_HLL: return pick<TY, RECON, RS_HLL>(ct, comp);
+    case RS_LLF: return pick<TY, RECON, RS_LLF>(ct, comp);
+  }
+  return nullptr;
+}
+template <int TY>
+StepKernelInfo info(int recon, int rsol, bool ct, bool comp) {
+  StepKernelInfo k{nullptr, StepSmem<TY>::BYTES, 32 * (TY + 2)};
+  switch (recon) {
+    case RECON_PLM: k.fn = pick_rs<TY, RECON_PLM>(rsol, ct, comp); break;
+    case RECON_PPM: k.fn = pick_rs<TY, RECON_PPM>(rsol, ct, comp); break;
+    case RECON_PLM_MINMOD: k.fn = pick_rs<TY, RECON_PLM_MINMOD>(rsol, ct, comp); break;
+  }
+  return k;
+}
+}  // namespace detail
+}  // namespace pmf

@@ -79,6 +79,9 @@ SIGNATURES = {
                             ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
     "pmfmhd_batch_destroy": ([_VP], ctypes.c_int),
     "pmfmhd_autotune": ([_VP, _GP, _P9, ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
+    "pmfmhd_set_tile": ([_VP, _GP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "pmfmhd_get_tile": ([_VP, _GP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                         ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
 }
 
 _lib = None
@@ -343,6 +346,20 @@ def run_glm(s: MHDState, nsteps: int, dt: float, ch: float, decay: float) -> MHD
 def autotune(s: MHDState) -> None:
     _check(lib().pmfmhd_autotune(context(s.device), ctypes.byref(s.grid), _p9(s.U), 1 if uses_ct(s) else 0,
                                  1 if s.resid is not None else 0, _stream()), "autotune")
+
+
+def set_tile(s: MHDState, rows: int, planes: int) -> None:
+    """Pin the CTA tile (owned rows, z-planes per chunk) used for this state's grid."""
+    _check(lib().pmfmhd_set_tile(context(s.device), ctypes.byref(s.grid), 1 if uses_ct(s) else 0,
+                                 1 if s.resid is not None else 0, int(rows), int(planes)), "set_tile")
+
+
+def get_tile(s: MHDState):
+    rows, planes = ctypes.c_int(), ctypes.c_int()
+    _check(lib().pmfmhd_get_tile(context(s.device), ctypes.byref(s.grid), 1 if uses_ct(s) else 0,
+                                 1 if s.resid is not None else 0, ctypes.byref(rows), ctypes.byref(planes)),
+           "get_tile")
+    return rows.value, planes.value
 
 
 def max_divb(s: MHDState) -> float:
