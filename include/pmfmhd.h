@@ -171,7 +171,7 @@ typedef struct pmfmhd_batch pmfmhd_batch;
 int pmfmhd_batch_create(pmfmhd_ctx* ctx, const pmfmhd_box* boxes, int nbox, pmfmhd_batch** out);
 int pmfmhd_batch_step(pmfmhd_batch* b, int nsteps, void* stream);
 /* Per-box results after the last step: time advanced, current-state index (0: U, 1: scratch),
- * last dt. Any pointer may be NULL. Blocking. */
+ * dt of the next step. Any pointer may be NULL. Blocking. */
 int pmfmhd_batch_query(pmfmhd_batch* b, double* t, int32_t* parity, float* dt);
 int pmfmhd_batch_destroy(pmfmhd_batch* b);
 

@@ -33,7 +33,7 @@ template <class T> __device__ __forceinline__ T block_reduce_max(T v) {
 }
 
 // max over cells of max_d(|v_d| + c_f,d)  (timestep.jl:4-14), one atomic per block
-__global__ void __launch_bounds__(AUX_THREADS) wavespeed_kernel(const CPtr9 U, int nc, Phys P,
+static __global__ void __launch_bounds__(AUX_THREADS) wavespeed_kernel(const CPtr9 U, int nc, Phys P,
                                                                 unsigned int* out_bits) {
   float m = 0.0f;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(AUX_THREADS) wavespeed_kernel(const CPtr9 U, i
 }
 
 // max |div B| by BC-aware centred differences, in FP64 (diagnostics.jl:6-20)
-__global__ void __launch_bounds__(AUX_THREADS) divb_kernel(const float* __restrict__ bx, const float* __restrict__ by,
+static __global__ void __launch_bounds__(AUX_THREADS) divb_kernel(const float* __restrict__ bx, const float* __restrict__ by,
                                                            const float* __restrict__ bz, int nx, int ny, int nz,
                                                            int bcx, int bcy, int bcz, double inv2dx,
                                                            unsigned long long* out_bits) {
@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(AUX_THREADS) divb_kernel(const float* __restri
 }
 
 // max face divergence of a CT face field, FP64 (ct.jl:176-185)
-__global__ void __launch_bounds__(AUX_THREADS) divb_face_kernel(const float* __restrict__ bxf,
+static __global__ void __launch_bounds__(AUX_THREADS) divb_face_kernel(const float* __restrict__ bxf,
                                                                 const float* __restrict__ byf,
                                                                 const float* __restrict__ bzf, int nx, int ny,
                                                                 int nz, double invdx,
@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(AUX_THREADS) divb_face_kernel(const float* __r
 }
 
 // Deterministic FP64 field sums: per-block partials (fixed order), then one block folds them.
-__global__ void __launch_bounds__(AUX_THREADS) totals_partial_kernel(const CPtr9 U, int nc,
+static __global__ void __launch_bounds__(AUX_THREADS) totals_partial_kernel(const CPtr9 U, int nc,
                                                                      double* partial) {
   __shared__ double red[AUX_THREADS / 32][8];
   double s[8];
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(AUX_THREADS) totals_partial_kernel(const CPtr9
     partial[blockIdx.x * 8 + threadIdx.x] = t;
   }
 }
-__global__ void totals_final_kernel(const double* partial, int nblocks, double scale, double* out) {
+static __global__ void totals_final_kernel(const double* partial, int nblocks, double scale, double* out) {
   if (threadIdx.x < 8) {
     double t = 0.0;
     for (int b = 0; b < nblocks; ++b) t += partial[b * 8 + threadIdx.x];
@@ -140,88 +140,100 @@ __device__ __forceinline__ float gs05(float Ea0, float Eam, float Eb0, float Ebm
 enum { CT_BXF = 0, CT_BYF, CT_BZF, CT_MFX, CT_MFY, CT_MFZ, CT_FXBY, CT_FXBZ, CT_FYBX, CT_FYBZ, CT_FZBX, CT_FZBY,
        CT_ECX, CT_ECY, CT_ECZ, CT_EX, CT_EY, CT_EZ, CT_RBX, CT_RBY, CT_RBZ, CT_NSLOT };
 
-// edge EMFs from the lower-face fluxes and cell EMFs (ct.jl:71-93)
-__global__ void __launch_bounds__(AUX_THREADS) ct_emf_kernel(float* __restrict__ ct, int nx, int ny, int nz) {
+// edge EMFs of cell c from the lower-face fluxes and cell EMFs (ct.jl:71-93)
+__device__ __forceinline__ void ct_emf_cell(float* __restrict__ ct, int nx, int ny, int nz, int c) {
   const int nxy = nx * ny, nc = nxy * nz;
   const float* W = ct;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
-    const int i = c % nx, j = (c / nx) % ny, k = c / nxy;
-    const int im = wrap_dec(i, nx), jm = wrap_dec(j, ny), km = wrap_dec(k, nz);
-    const int cim = k * nxy + j * nx + im, cjm = k * nxy + jm * nx + i, ckm = km * nxy + j * nx + i;
-    const int cimjm = k * nxy + jm * nx + im, cjmkm = km * nxy + jm * nx + i, ckmim = km * nxy + j * nx + im;
-    auto w = [&](int s, int x) { return __ldg(W + (size_t)s * nc + x); };
-    ct[(size_t)CT_EZ * nc + c] =
-        gs05(-w(CT_FXBY, c), -w(CT_FXBY, cjm), w(CT_FYBX, c), w(CT_FYBX, cim), w(CT_MFX, c), w(CT_MFX, cjm),
-             w(CT_MFY, c), w(CT_MFY, cim), w(CT_ECZ, c), w(CT_ECZ, cim), w(CT_ECZ, cjm), w(CT_ECZ, cimjm));
-    ct[(size_t)CT_EX * nc + c] =
-        gs05(-w(CT_FYBZ, c), -w(CT_FYBZ, ckm), w(CT_FZBY, c), w(CT_FZBY, cjm), w(CT_MFY, c), w(CT_MFY, ckm),
-             w(CT_MFZ, c), w(CT_MFZ, cjm), w(CT_ECX, c), w(CT_ECX, cjm), w(CT_ECX, ckm), w(CT_ECX, cjmkm));
-    ct[(size_t)CT_EY * nc + c] =
-        gs05(-w(CT_FZBX, c), -w(CT_FZBX, cim), w(CT_FXBZ, c), w(CT_FXBZ, ckm), w(CT_MFZ, c), w(CT_MFZ, cim),
-             w(CT_MFX, c), w(CT_MFX, ckm), w(CT_ECY, c), w(CT_ECY, ckm), w(CT_ECY, cim), w(CT_ECY, ckmim));
-  }
+  const int i = c % nx, j = (c / nx) % ny, k = c / nxy;
+  const int im = wrap_dec(i, nx), jm = wrap_dec(j, ny), km = wrap_dec(k, nz);
+  const int cim = k * nxy + j * nx + im, cjm = k * nxy + jm * nx + i, ckm = km * nxy + j * nx + i;
+  const int cimjm = k * nxy + jm * nx + im, cjmkm = km * nxy + jm * nx + i, ckmim = km * nxy + j * nx + im;
+  auto w = [&](int s, int x) { return __ldg(W + (size_t)s * nc + x); };
+  ct[(size_t)CT_EZ * nc + c] =
+      gs05(-w(CT_FXBY, c), -w(CT_FXBY, cjm), w(CT_FYBX, c), w(CT_FYBX, cim), w(CT_MFX, c), w(CT_MFX, cjm),
+           w(CT_MFY, c), w(CT_MFY, cim), w(CT_ECZ, c), w(CT_ECZ, cim), w(CT_ECZ, cjm), w(CT_ECZ, cimjm));
+  ct[(size_t)CT_EX * nc + c] =
+      gs05(-w(CT_FYBZ, c), -w(CT_FYBZ, ckm), w(CT_FZBY, c), w(CT_FZBY, cjm), w(CT_MFY, c), w(CT_MFY, ckm),
+           w(CT_MFZ, c), w(CT_MFZ, cjm), w(CT_ECX, c), w(CT_ECX, cjm), w(CT_ECX, ckm), w(CT_ECX, cjmkm));
+  ct[(size_t)CT_EY * nc + c] =
+      gs05(-w(CT_FZBX, c), -w(CT_FZBX, cim), w(CT_FXBZ, c), w(CT_FXBZ, ckm), w(CT_MFZ, c), w(CT_MFZ, cim),
+           w(CT_MFX, c), w(CT_MFX, ckm), w(CT_ECY, c), w(CT_ECY, ckm), w(CT_ECY, cim), w(CT_ECY, ckmim));
 }
 
-// face update by the discrete curl of the edge EMFs, plain or Kahan (ct.jl:96-129)
+static __global__ void __launch_bounds__(AUX_THREADS) ct_emf_kernel(float* __restrict__ ct, int nx, int ny, int nz) {
+  const int nc = nx * ny * nz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) ct_emf_cell(ct, nx, ny, nz, c);
+}
+
+// face update of cell c by the discrete curl of the edge EMFs, plain or Kahan (ct.jl:96-129)
 template <bool COMP>
-__global__ void __launch_bounds__(AUX_THREADS) ct_face_kernel(float* __restrict__ ct, int nx, int ny, int nz,
-                                                              float dtdx) {
+__device__ __forceinline__ void ct_face_cell(float* __restrict__ ct, int nx, int ny, int nz, float dtdx, int c) {
   const int nxy = nx * ny, nc = nxy * nz;
   const float* ex = ct + (size_t)CT_EX * nc;
   const float* ey = ct + (size_t)CT_EY * nc;
   const float* ez = ct + (size_t)CT_EZ * nc;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
-    const int i = c % nx, j = (c / nx) % ny, k = c / nxy;
-    const int ip = k * nxy + j * nx + wrap_inc(i, nx), jp = k * nxy + wrap_inc(j, ny) * nx + i,
-              kp = wrap_inc(k, nz) * nxy + j * nx + i;
-    const float dbx = dtdx * ((ez[jp] - ez[c]) - (ey[kp] - ey[c]));
-    const float dby = dtdx * ((ex[kp] - ex[c]) - (ez[ip] - ez[c]));
-    const float dbz = dtdx * ((ey[ip] - ey[c]) - (ex[jp] - ex[c]));
-    float* bxf = ct + (size_t)CT_BXF * nc;
-    float* byf = ct + (size_t)CT_BYF * nc;
-    float* bzf = ct + (size_t)CT_BZF * nc;
-    if (COMP) {
-      float* rbx = ct + (size_t)CT_RBX * nc;
-      float* rby = ct + (size_t)CT_RBY * nc;
-      float* rbz = ct + (size_t)CT_RBZ * nc;
-      float r = rbx[c];
-      bxf[c] = comp_add(bxf[c], -dbx, r);
-      rbx[c] = r;
-      r = rby[c];
-      byf[c] = comp_add(byf[c], -dby, r);
-      rby[c] = r;
-      r = rbz[c];
-      bzf[c] = comp_add(bzf[c], -dbz, r);
-      rbz[c] = r;
-    } else {
-      bxf[c] -= dbx;
-      byf[c] -= dby;
-      bzf[c] -= dbz;
-    }
+  const int i = c % nx, j = (c / nx) % ny, k = c / nxy;
+  const int ip = k * nxy + j * nx + wrap_inc(i, nx), jp = k * nxy + wrap_inc(j, ny) * nx + i,
+            kp = wrap_inc(k, nz) * nxy + j * nx + i;
+  const float dbx = dtdx * ((ez[jp] - ez[c]) - (ey[kp] - ey[c]));
+  const float dby = dtdx * ((ex[kp] - ex[c]) - (ez[ip] - ez[c]));
+  const float dbz = dtdx * ((ey[ip] - ey[c]) - (ex[jp] - ex[c]));
+  float* bxf = ct + (size_t)CT_BXF * nc;
+  float* byf = ct + (size_t)CT_BYF * nc;
+  float* bzf = ct + (size_t)CT_BZF * nc;
+  if (COMP) {
+    float* rbx = ct + (size_t)CT_RBX * nc;
+    float* rby = ct + (size_t)CT_RBY * nc;
+    float* rbz = ct + (size_t)CT_RBZ * nc;
+    float r = rbx[c];
+    bxf[c] = comp_add(bxf[c], -dbx, r);
+    rbx[c] = r;
+    r = rby[c];
+    byf[c] = comp_add(byf[c], -dby, r);
+    rby[c] = r;
+    r = rbz[c];
+    bzf[c] = comp_add(bzf[c], -dbz, r);
+    rbz[c] = r;
+  } else {
+    bxf[c] -= dbx;
+    byf[c] -= dby;
+    bzf[c] -= dbz;
   }
 }
 
-// cell B = face average (ct.jl:132-143), then the new state's max signal speed
-__global__ void __launch_bounds__(AUX_THREADS) ct_bcc_kernel(const float* __restrict__ ct, const MPtr9 Un, int nx,
-                                                             int ny, int nz, Phys P, unsigned int* smax_bits) {
+template <bool COMP>
+static __global__ void __launch_bounds__(AUX_THREADS) ct_face_kernel(float* __restrict__ ct, int nx, int ny, int nz,
+                                                              float dtdx) {
+  const int nc = nx * ny * nz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
+    ct_face_cell<COMP>(ct, nx, ny, nz, dtdx, c);
+}
+
+// cell B of cell c = face average (ct.jl:132-143); returns the new state's signal speed
+__device__ __forceinline__ float ct_bcc_cell(const float* __restrict__ ct, const MPtr9& Un, int nx, int ny, int nz,
+                                             const Phys& P, bool want_speed, int c) {
   const int nxy = nx * ny, nc = nxy * nz;
   const float* bxf = ct + (size_t)CT_BXF * nc;
   const float* byf = ct + (size_t)CT_BYF * nc;
   const float* bzf = ct + (size_t)CT_BZF * nc;
+  const int i = c % nx, j = (c / nx) % ny, k = c / nxy;
+  const float bx = 0.5f * (bxf[c] + bxf[k * nxy + j * nx + wrap_inc(i, nx)]);
+  const float by = 0.5f * (byf[c] + byf[k * nxy + wrap_inc(j, ny) * nx + i]);
+  const float bz = 0.5f * (bzf[c] + bzf[wrap_inc(k, nz) * nxy + j * nx + i]);
+  Un.p[5][c] = bx;
+  Un.p[6][c] = by;
+  Un.p[7][c] = bz;
+  if (!want_speed) return 0.0f;
+  F9 u{{Un.p[0][c], Un.p[1][c], Un.p[2][c], Un.p[3][c], Un.p[4][c], bx, by, bz, 0.0f}};
+  return cell_wavespeed(u, P);
+}
+
+static __global__ void __launch_bounds__(AUX_THREADS) ct_bcc_kernel(const float* __restrict__ ct, const MPtr9 Un, int nx,
+                                                             int ny, int nz, Phys P, unsigned int* smax_bits) {
+  const int nc = nx * ny * nz;
   float m = 0.0f;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
-    const int i = c % nx, j = (c / nx) % ny, k = c / nxy;
-    const float bx = 0.5f * (bxf[c] + bxf[k * nxy + j * nx + wrap_inc(i, nx)]);
-    const float by = 0.5f * (byf[c] + byf[k * nxy + wrap_inc(j, ny) * nx + i]);
-    const float bz = 0.5f * (bzf[c] + bzf[wrap_inc(k, nz) * nxy + j * nx + i]);
-    Un.p[5][c] = bx;
-    Un.p[6][c] = by;
-    Un.p[7][c] = bz;
-    if (smax_bits != nullptr) {
-      F9 u{{Un.p[0][c], Un.p[1][c], Un.p[2][c], Un.p[3][c], Un.p[4][c], bx, by, bz, 0.0f}};
-      m = fmaxf(m, cell_wavespeed(u, P));
-    }
-  }
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
+    m = fmaxf(m, ct_bcc_cell(ct, Un, nx, ny, nz, P, smax_bits != nullptr, c));
   if (smax_bits != nullptr) {
     m = block_reduce_max(m);
     if (threadIdx.x == 0) atomicMax(smax_bits, __float_as_uint(m));
@@ -229,7 +241,7 @@ __global__ void __launch_bounds__(AUX_THREADS) ct_bcc_kernel(const float* __rest
 }
 
 // faces = discrete curl of an edge potential (ct.jl:310-320)
-__global__ void __launch_bounds__(AUX_THREADS) ct_curl_kernel(const float* __restrict__ Ax,
+static __global__ void __launch_bounds__(AUX_THREADS) ct_curl_kernel(const float* __restrict__ Ax,
                                                               const float* __restrict__ Ay,
                                                               const float* __restrict__ Az, float* __restrict__ ct,
                                                               int nx, int ny, int nz, float invdx) {
@@ -248,7 +260,7 @@ __global__ void __launch_bounds__(AUX_THREADS) ct_curl_kernel(const float* __res
 }
 
 // cell B <- face average, E keeps the thermal pressure, psi <- 0 (ct.jl:205-219)
-__global__ void __launch_bounds__(AUX_THREADS) ct_cell_from_faces_kernel(const float* __restrict__ ct,
+static __global__ void __launch_bounds__(AUX_THREADS) ct_cell_from_faces_kernel(const float* __restrict__ ct,
                                                                          const MPtr9 U, int nx, int ny, int nz) {
   const int nxy = nx * ny, nc = nxy * nz;
   const float* bxf = ct + (size_t)CT_BXF * nc;

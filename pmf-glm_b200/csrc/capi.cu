@@ -13,57 +13,27 @@
 #include "../../include/pmfmhd.h"
 #include "aux_kernels.cuh"
 #include "dispatch.h"
+#include "host_internal.h"
 #include "step_kernel.cuh"
 
 using namespace pmf;
+using namespace pmf::host;
 
 namespace {
-
-thread_local std::string g_last_cuda;
-
-#define PMF_CK(call)                                                              \
-  do {                                                                            \
-    cudaError_t e_ = (call);                                                      \
-    if (e_ != cudaSuccess) {                                                      \
-      g_last_cuda = std::string(#call) + ": " + cudaGetErrorString(e_);            \
-      return PMFMHD_ECUDA;                                                        \
-    }                                                                             \
-  } while (0)
-
 constexpr int kTotBlocksMax = 1024;
-
-struct TuneKey {
-  int nx, ny, nz, ct, comp, recon, rsol;
-  bool operator<(const TuneKey& o) const {
-    return std::tie(nx, ny, nz, ct, comp, recon, rsol) < std::tie(o.nx, o.ny, o.nz, o.ct, o.comp, o.recon, o.rsol);
-  }
-};
-struct Tune {
-  int ty, tz;
-};
-
-struct GraphEntry {
-  std::vector<unsigned char> key;
-  cudaGraphExec_t exec;
-};
-
 }  // namespace
 
-struct pmfmhd_ctx {
-  int device = 0;
-  int sms = 148;
-  unsigned int* d_smax = nullptr;           // bits of the last step's max signal speed
-  unsigned long long* d_u64 = nullptr;      // bits of an FP64 max
-  double* d_partial = nullptr;              // totals partials
-  double* d_tot = nullptr;                  // totals
-  unsigned char* h_pin = nullptr;           // pinned host landing area
-  cudaStream_t cap = nullptr;               // stream used to record graphs
-  std::map<TuneKey, Tune> tune;
-  std::vector<GraphEntry> graphs;
-  std::mutex mu;
-};
+namespace pmf {
+namespace host {
+std::string& last_cuda_error() {
+  thread_local std::string e;
+  return e;
+}
+}  // namespace host
+}  // namespace pmf
 
-namespace {
+namespace pmf {
+namespace host {
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
@@ -215,7 +185,8 @@ int read_smax(pmfmhd_ctx* c, float* out, cudaStream_t s) {
   return PMFMHD_OK;
 }
 
-}  // namespace
+}  // namespace host
+}  // namespace pmf
 
 extern "C" {
 
@@ -235,7 +206,7 @@ const char* pmfmhd_strerror(int code) {
   return "unknown error";
 }
 
-const char* pmfmhd_last_cuda_error(void) { return g_last_cuda.c_str(); }
+const char* pmfmhd_last_cuda_error(void) { return last_cuda_error().c_str(); }
 
 int pmfmhd_create(int device, pmfmhd_ctx** out) {
   if (out == nullptr) return PMFMHD_EINVAL;
@@ -248,7 +219,7 @@ int pmfmhd_create(int device, pmfmhd_ctx** out) {
       cudaMalloc(&c->d_partial, sizeof(double) * 8 * kTotBlocksMax) != cudaSuccess ||
       cudaMalloc(&c->d_tot, sizeof(double) * 8) != cudaSuccess || cudaMallocHost(&c->h_pin, 256) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking) != cudaSuccess) {
-    g_last_cuda = cudaGetErrorString(cudaGetLastError());
+    last_cuda_error() = cudaGetErrorString(cudaGetLastError());
     pmfmhd_destroy(c);
     return PMFMHD_ENOMEM;
   }
@@ -443,9 +414,10 @@ int pmfmhd_run_glm(pmfmhd_ctx* c, const pmfmhd_grid* g, float* const U[9], float
     cudaMemsetAsync(c->d_smax, 0, sizeof(unsigned int), c->cap);
     int lrc = launch_step(c, g, a, t, false, comp, c->cap);
     if (lrc != PMFMHD_OK) {
-      cudaGraph_t dead;
+      cudaGraph_t dead = nullptr;
       cudaStreamEndCapture(c->cap, &dead);
       if (dead) cudaGraphDestroy(dead);
+      cudaGetLastError();  // leave no error from the abandoned capture behind
       return lrc;
     }
   }
@@ -455,7 +427,7 @@ int pmfmhd_run_glm(pmfmhd_ctx* c, const pmfmhd_grid* g, float* const U[9], float
   cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) {
-    g_last_cuda = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+    last_cuda_error() = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
     return PMFMHD_ECUDA;
   }
   if (c->graphs.size() >= 16) {

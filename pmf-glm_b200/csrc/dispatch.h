@@ -4,7 +4,9 @@
 
 namespace pmf {
 struct StepArgs;
+struct BoxStep;
 using StepKernel = void (*)(const StepArgs);
+using BatchKernel = void (*)(const BoxStep*, int, long long);
 
 struct StepKernelInfo {
   StepKernel fn;      // null if the combination is not instantiated
@@ -17,4 +19,6 @@ constexpr int kTileRows[] = {4, 8, 14};
 constexpr int kNumTileRows = 3;
 
 StepKernelInfo step_kernel_info(int ty, int recon, int rsol, bool ct, bool comp);
+// The many-box form of the same kernel (same shared memory and block size).
+BatchKernel batch_kernel(int ty, int recon, int rsol, bool ct, bool comp);
 }  // namespace pmf

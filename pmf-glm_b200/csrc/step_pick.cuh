@@ -10,6 +10,29 @@ StepKernel pick(bool ct, bool comp) {
   if (ct) return comp ? mhd_step_kernel<TY, RECON, RSOL, true, true> : mhd_step_kernel<TY, RECON, RSOL, true, false>;
   return comp ? mhd_step_kernel<TY, RECON, RSOL, false, true> : mhd_step_kernel<TY, RECON, RSOL, false, false>;
 }
+template <int TY, int RECON, int RSOL>
+BatchKernel pick_batch(bool ct, bool comp) {
+  if (ct) return comp ? mhd_batch_kernel<TY, RECON, RSOL, true, true> : mhd_batch_kernel<TY, RECON, RSOL, true, false>;
+  return comp ? mhd_batch_kernel<TY, RECON, RSOL, false, true> : mhd_batch_kernel<TY, RECON, RSOL, false, false>;
+}
+template <int TY, int RECON>
+BatchKernel pick_batch_rs(int rsol, bool ct, bool comp) {
+  switch (rsol) {
+    case RS_HLLD: return pick_batch<TY, RECON, RS_HLLD>(ct, comp);
+    case RS_HLL: return pick_batch<TY, RECON, RS_HLL>(ct, comp);
+    case RS_LLF: return pick_batch<TY, RECON, RS_LLF>(ct, comp);
+  }
+  return nullptr;
+}
+template <int TY>
+BatchKernel batch(int recon, int rsol, bool ct, bool comp) {
+  switch (recon) {
+    case RECON_PLM: return pick_batch_rs<TY, RECON_PLM>(rsol, ct, comp);
+    case RECON_PPM: return pick_batch_rs<TY, RECON_PPM>(rsol, ct, comp);
+    case RECON_PLM_MINMOD: return pick_batch_rs<TY, RECON_PLM_MINMOD>(rsol, ct, comp);
+  }
+  return nullptr;
+}
 template <int TY, int RECON>
 StepKernel pick_rs(int rsol, bool ct, bool comp) {
   switch (rsol) {

@@ -5,4 +5,7 @@ namespace pmf {
 StepKernelInfo step_kernel_info_ty8(int recon, int rsol, bool ct, bool comp) {
   return detail::info<8>(recon, rsol, ct, comp);
 }
+BatchKernel batch_kernel_ty8(int recon, int rsol, bool ct, bool comp) {
+  return detail::batch<8>(recon, rsol, ct, comp);
+}
 }  // namespace pmf

@@ -432,7 +432,7 @@ def ct_faces_from_cells(s: MHDState) -> dict:
     Fx = bx * np.exp(-1j * thx) / np.cos(thx)
     Fy = by * np.exp(-1j * thy) / np.cos(thy)
     Fz = bz * np.exp(-1j * thz) / np.cos(thz)
-    faces = [np.fft.irfftn(F, s=(nz, ny, nx)).ravel() for F in (Fx, Fy, Fz)]
+    faces = [np.fft.irfftn(F, s=(nz, ny, nx), axes=(0, 1, 2)).ravel() for F in (Fx, Fy, Fz)]
     dev = torch.device("cuda", s.device)
     s.ct.slot(18).zero_(); s.ct.slot(19).zero_(); s.ct.slot(20).zero_()
     for d in range(3):
