@@ -120,3 +120,20 @@ def turbulent_box(n, seed=0, mach=0.5, beta=1.0, rho_sigma=0.1, lognormal=False,
                   B[0].ravel(), B[1].ravel(), B[2].ravel(), np.zeros(n ** 3)])
     U = prim2cons(q, gamma).astype(dtype)
     return {"U": U, "A_edge": A_edge, "faces": faces, "p0": p0}
+
+
+def batch_mix(nbox=64, seed=2024, sizes=(32, 48, 64, 96, 128), weights=(5, 4, 3, 2, 1)):
+    """Box specifications of the batched workload: side lengths drawn from `sizes` with
+    uneven weights, plasma beta log-uniform in [0.01, 10], magnetic spectral index
+    uniform in [-2.9, 2], cutoff uniform in [N/8, N/3], GLM and CT alternating at random,
+    and a seed per box. Deterministic in `seed`."""
+    rng = np.random.default_rng(seed)
+    p = np.asarray(weights, dtype=np.float64)
+    p /= p.sum()
+    specs = []
+    for i in range(nbox):
+        n = int(rng.choice(sizes, p=p))
+        specs.append({"n": n, "beta": float(10 ** rng.uniform(-2.0, 1.0)), "b_index": float(rng.uniform(-2.9, 2.0)),
+                      "kc": float(rng.uniform(n / 8, n / 3)), "seed": int(seed + 101 * i),
+                      "ct": bool(rng.integers(0, 2))})
+    return specs
