@@ -84,7 +84,7 @@ int aux_blocks(const pmfmhd_ctx* c, long long nc) {
 // equal share of the (column, plane) space, but never less than `tz` planes).
 Tune default_tune(const pmfmhd_ctx*, const pmfmhd_grid* g) {
   Tune t;
-  t.ty = g->ny >= 14 ? 14 : (g->ny >= 8 ? 8 : 4);
+  t.ty = g->ny >= 13 ? 13 : (g->ny >= 8 ? 8 : 5);
   t.tz = 16;
   return t;
 }
@@ -473,7 +473,7 @@ int pmfmhd_autotune(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9]
   float best_ms = 1e30f;
   std::vector<int> tzs = {8, 32};
   for (int ty : kTileRows) {
-    if (ty > 4 && g->ny < ty) continue;
+    if (ty > 5 && g->ny < ty) continue;
     for (int tz : tzs) {
       Tune t{ty, tz};
       float ms_sum = 0.0f;

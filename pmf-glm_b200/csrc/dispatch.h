@@ -15,7 +15,7 @@ struct StepKernelInfo {
 };
 
 // Rows per CTA that are instantiated (tile candidates for the autotuner).
-constexpr int kTileRows[] = {4, 8, 14};
+constexpr int kTileRows[] = {5, 8, 13};
 constexpr int kNumTileRows = 3;
 
 StepKernelInfo step_kernel_info(int ty, int recon, int rsol, bool ct, bool comp);

@@ -2,28 +2,28 @@
 #include "dispatch.h"
 
 namespace pmf {
-StepKernelInfo step_kernel_info_ty4(int recon, int rsol, bool ct, bool comp);
+StepKernelInfo step_kernel_info_ty5(int recon, int rsol, bool ct, bool comp);
 StepKernelInfo step_kernel_info_ty8(int recon, int rsol, bool ct, bool comp);
-StepKernelInfo step_kernel_info_ty14(int recon, int rsol, bool ct, bool comp);
+StepKernelInfo step_kernel_info_ty13(int recon, int rsol, bool ct, bool comp);
 
-BatchKernel batch_kernel_ty4(int recon, int rsol, bool ct, bool comp);
+BatchKernel batch_kernel_ty5(int recon, int rsol, bool ct, bool comp);
 BatchKernel batch_kernel_ty8(int recon, int rsol, bool ct, bool comp);
-BatchKernel batch_kernel_ty14(int recon, int rsol, bool ct, bool comp);
+BatchKernel batch_kernel_ty13(int recon, int rsol, bool ct, bool comp);
 
 BatchKernel batch_kernel(int ty, int recon, int rsol, bool ct, bool comp) {
   switch (ty) {
-    case 4: return batch_kernel_ty4(recon, rsol, ct, comp);
+    case 5: return batch_kernel_ty5(recon, rsol, ct, comp);
     case 8: return batch_kernel_ty8(recon, rsol, ct, comp);
-    case 14: return batch_kernel_ty14(recon, rsol, ct, comp);
+    case 13: return batch_kernel_ty13(recon, rsol, ct, comp);
   }
   return nullptr;
 }
 
 StepKernelInfo step_kernel_info(int ty, int recon, int rsol, bool ct, bool comp) {
   switch (ty) {
-    case 4: return step_kernel_info_ty4(recon, rsol, ct, comp);
+    case 5: return step_kernel_info_ty5(recon, rsol, ct, comp);
     case 8: return step_kernel_info_ty8(recon, rsol, ct, comp);
-    case 14: return step_kernel_info_ty14(recon, rsol, ct, comp);
+    case 13: return step_kernel_info_ty13(recon, rsol, ct, comp);
   }
   return StepKernelInfo{nullptr, 0, 0};
 }

@@ -6,13 +6,13 @@
 //   U' = U + dt/dx * (((Fxl-Fxh) + (Fyl-Fyh)) + (Fzl-Fzh)),  psi' *= decay.
 //
 // Decomposition (B200-specific, not the reference's 4^3 cube): one CTA owns a column of
-// 30 x TY cells in (x, y) and a chunk of planes in z, and marches through the chunk one
-// z-plane at a time.
-//   * warp w <-> row y0+w-1 (w = 0 and w = TY+1 are the y-halo rows); lane l <-> column
-//     x0+l-1 (lanes 0 and 31 are the x-halo cells). Each thread computes the Hancock state
-//     of its own cell once per plane.
-//   * x-faces are solved in registers: the left state comes from lane l-1 by __shfl_up,
-//     and the upper-face flux of a cell from lane l+1 by __shfl_down.
+// 32 x TY cells in (x, y) and streams through a range of z-planes one plane at a time.
+//   * row warps w = 0..TY+1 <-> rows y0+w-1 (w = 0 and TY+1 are the y-halo rows); lane l
+//     <-> column x0+l. One more "halo warp" computes, per owned row, the two x-halo cells
+//     x0-1 and x0+32. Every thread computes the Hancock state of its cell once per plane.
+//   * x-faces are solved in registers: lane l solves the face below its cell with the left
+//     state from lane l-1 by __shfl_up (lane 0 takes the left halo cell's state from shared
+//     memory); the face above lane 31 is solved by the halo warp.
 //   * y-faces exchange one 9-float state per thread through shared memory.
 //   * z-faces never leave registers: each thread keeps the upper z-face state, the lower
 //     z-face flux and the x/y flux divergence of the previous plane of its own column, so
@@ -20,15 +20,18 @@
 // Primitives of planes p-1, p, p+1 (with a 2-cell ring) live in a 3-slot shared ring; the
 // raw conserved plane p+2 is prefetched into a staging buffer by cp.async while plane p is
 // computed. Each face is solved exactly once per CTA; the only recomputation is the Hancock
-// state of the one-cell halo ring (~1.3x the owned cells) and the halo rows' y-faces.
+// state of the one-cell halo ring and the halo rows' y-faces.
 // The new state's max signal speed (timestep.jl:4-14) is reduced in the same pass.
 #pragma once
 #include "physics.cuh"
 
 namespace pmf {
 
-constexpr int TILE_X = 30;  // owned columns per CTA (32 lanes minus 2 halo lanes)
-constexpr int PLANE_W = 34; // primitive ring width: x0-2 .. x0+31
+constexpr int TILE_X = 32;  // owned columns per CTA: one warp lane per column
+constexpr int PLANE_W = 36; // primitive ring width: x0-2 .. x0+33
+
+// Threads per CTA: TY+2 row warps and the halo warp.
+template <int TY> constexpr int step_threads() { return 32 * (TY + 3); }
 
 // Number of CT workspace arrays written by the Godunov stage (reference CTState slots 4-15).
 constexpr int CT_NWORK = 12;
@@ -55,7 +58,9 @@ struct StepSmem {
   static constexpr int STAGE = 9 * PP;              // raw conserved plane
   static constexpr int PRIM = 3 * 9 * PP;           // 3-plane primitive ring
   static constexpr int YB = (TY + 1) * 9 * 32;      // y-face states / fluxes
-  static constexpr int FLOATS = STAGE + PRIM + 2 * YB;
+  static constexpr int XB = TY * 9;                 // one x-face state or flux per owned row
+  static constexpr int ZC = TY * 18 * 32;           // per owned thread: upper z state, lower z flux
+  static constexpr int FLOATS = STAGE + PRIM + 2 * YB + 3 * XB + ZC;
   static constexpr size_t BYTES = sizeof(float) * FLOATS;
 };
 
@@ -72,12 +77,16 @@ template <int TY, int RECON, int RSOL, bool CT, bool COMP>
 __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, int z0, int z1, float* smem,
                                              float& smax) {
   using S = StepSmem<TY>;
-  constexpr int NT = 32 * (TY + 2);
+  constexpr int NT = step_threads<TY>();
   constexpr int PP = S::PP;
   float* stage = smem;
   float* prim = smem + S::STAGE;
   float* ybuf = prim + S::PRIM;
   float* fybuf = ybuf + S::YB;
+  float* xleft = fybuf + S::YB;    // [row][9] upper x state of the left halo cell
+  float* xright = xleft + S::XB;   // [row][9] upper x state of lane 31
+  float* fxright = xright + S::XB; // [row][9] flux through the face above lane 31
+  float* zcarry = fxright + S::XB; // [row][18][32] upper z state and lower z flux of plane p-1
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5;
@@ -90,9 +99,15 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   const Phys P = a.P;
   const float g = P.gamma;
 
-  const int x = x0 + lane - 1, y = y0 + w - 1;
-  const bool own = lane >= 1 && lane <= TILE_X && w >= 1 && w <= TY && x < nx && y < ny;
+  // row warps: cell (x0+lane, y0+w-1); halo warp lane t < 2*TY: row t/2, left (x0-1) or
+  // right (x0+32) halo cell
+  const bool halo_warp = w == TY + 2;
+  const int hrow = lane >> 1, hside = lane & 1;
+  const bool halo_act = halo_warp && lane < 2 * TY;
+  const int x = halo_warp ? (hside ? x0 + TILE_X : x0 - 1) : x0 + lane;
+  const int y = halo_warp ? y0 + hrow : y0 + w - 1;
   const bool row_own = w >= 1 && w <= TY;
+  const bool own = row_own && x < nx && y < ny;
 
   // Source cell of staged-plane entry e (row r, column c) of logical plane zp, with BCs.
   auto issue_plane = [&](int zp) {
@@ -151,11 +166,24 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   __syncthreads();
   issue_plane(z0);
 
-  // Per-column carries across planes (owned rows only).
-  F9 zR;      // upper z-face state of plane p-1
-  F9 Fzc;     // flux through the lower z-face of plane p-1
+  // Per-column carries across planes (owned rows only): the upper z-face state and the
+  // lower z-face flux of plane p-1 live in this thread's private slots of `zcarry`; the
+  // x/y divergence of plane p-1 stays in registers.
   F9 dUxy;    // (Fxl - Fxh) + (Fyl - Fyh) of plane p-1
-  const int r0 = w + 1, c0 = lane + 1;  // this thread's cell in the staged plane
+  float* zc = zcarry + (row_own ? (w - 1) : 0) * 18 * 32 + lane;
+  auto zc_store = [&](int off, const F9& v) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) zc[(off + i) * 32] = v[i];
+  };
+  auto zc_load = [&](int off) {
+    F9 v;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) v[i] = zc[(off + i) * 32];
+    return v;
+  };
+  // this thread's cell in the staged plane (halo lanes beyond 2*TY read a valid dummy cell)
+  const int r0 = halo_warp ? (halo_act ? hrow + 2 : 2) : w + 1;
+  const int c0 = halo_warp ? (hside ? TILE_X + 2 : 1) : lane + 2;
 
   // Conservative update of cell (x, y, pz) from its x/y divergence and its two z fluxes.
   auto update_cell = [&](int pz, const F9& dxy, const F9& flo, const F9& fhi) {
@@ -211,8 +239,10 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     __syncthreads();
     if (p + 2 <= z1 + 1) issue_plane(p + 2);
 
-    // plane z0-1 only feeds the lower z-face of the chunk: the y-halo rows skip it
+    // plane z0-1 only feeds the lower z-face of the chunk: only the owned rows need it
     if (p == z0 - 1 && !row_own) continue;
+    // the halo warp only works on owned planes
+    if (halo_warp && !(p >= z0 && p < z1)) continue;
 
     // ---- Hancock half step of this thread's cell in plane p ------------------------------
     const float* pm = slot(p - 1);
@@ -246,11 +276,11 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       }
     }
     if (p == z0 - 1) {
-      zR = face_hi<RECON>(mh, oz);
+      zc_store(0, face_hi<RECON>(mh, oz));
       continue;
     }
     // y-halo row 0 and the owned rows publish their upper y state for the face above
-    if (mid && w <= TY) {
+    if (mid && w <= TY) {  // row warps 0..TY (the halo warp is w = TY+2)
       const F9 yR = face_hi<RECON>(mh, oy);
 #pragma unroll
       for (int i = 0; i < 9; ++i) ybuf[(w * 9 + i) * 32 + lane] = yR[i];
@@ -259,14 +289,14 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       // ---- z-face p-1/2: left = carried upper z state of p-1, right = lower z state of p --
       F9 Fz;
       {
-        F9 L = zR, R = face_lo<RECON>(mh, oz);
+        F9 L = zc_load(0), R = face_lo<RECON>(mh, oz);
         if constexpr (CT) {
           const float bn = face_bn(2, p);
           L[7] = bn; R[7] = bn;
         }
         Fz = riemann<2, RSOL, CT>(L, R, ch, P);
       }
-      zR = face_hi<RECON>(mh, oz);
+      zc_store(0, face_hi<RECON>(mh, oz));
       if constexpr (CT) {
         if (own && mid) {
           a.work[2][cell_p] = Fz[0];
@@ -274,23 +304,47 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
           a.work[8][cell_p] = Fz[6];
         }
       }
-      if (p > z0 && own) update_cell(p - 1, dUxy, Fzc, Fz);
-      Fzc = Fz;
+      if (p > z0 && own) update_cell(p - 1, dUxy, zc_load(9), Fz);
+      zc_store(9, Fz);
     }
     if (!mid) continue;  // p == z1: only the last z-face and update were needed
 
-    // ---- x-faces: lane l solves the face between cells l-1 and l ------------------------
-    F9 dx_flux;  // (Fxl - Fxh) of this cell
-    if (row_own) {
-      F9 L, R = face_lo<RECON>(mh, ox);
+    // ---- x-face states at the tile edges go through shared memory ----------------------
+    if (row_own && lane == TILE_X - 1) {
       const F9 xR = face_hi<RECON>(mh, ox);
 #pragma unroll
-      for (int i = 0; i < 9; ++i) L[i] = __shfl_up_sync(0xffffffffu, xR[i], 1);
+      for (int i = 0; i < 9; ++i) xright[(w - 1) * 9 + i] = xR[i];
+    }
+    if (halo_act && hside == 0) {
+      const F9 xR = face_hi<RECON>(mh, ox);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) xleft[hrow * 9 + i] = xR[i];
+    }
+    __syncthreads();
+    // ---- x-faces: lane l of a row warp solves the face below column l (lane 0 against the
+    // left halo cell); the halo warp's right-side lanes solve the face above lane 31. Both
+    // go through this one call site, so a face shared by two tiles gets the same bits.
+    F9 xup;
+    {
+      const F9 xR = face_hi<RECON>(mh, ox);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) xup[i] = __shfl_up_sync(0xffffffffu, xR[i], 1);
+    }
+    F9 Fx;
+    if (row_own || (halo_act && hside == 1)) {
+      F9 L, R = face_lo<RECON>(mh, ox);
+#pragma unroll
+      for (int i = 0; i < 9; ++i)
+        L[i] = halo_warp ? xright[hrow * 9 + i] : (lane == 0 ? xleft[(w - 1) * 9 + i] : xup[i]);
       if constexpr (CT) {
         const float bn = face_bn(0, p);
         L[5] = bn; R[5] = bn;
       }
-      const F9 Fx = riemann<0, RSOL, CT>(L, R, ch, P);
+      Fx = riemann<0, RSOL, CT>(L, R, ch, P);
+      if (halo_warp) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) fxright[hrow * 9 + i] = Fx[i];
+      }
       if constexpr (CT) {
         if (own) {
           a.work[0][cell_p] = Fx[0];
@@ -298,13 +352,10 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
           a.work[4][cell_p] = Fx[7];
         }
       }
-#pragma unroll
-      for (int i = 0; i < 9; ++i) dx_flux[i] = Fx[i] - __shfl_down_sync(0xffffffffu, Fx[i], 1);
     }
-    __syncthreads();
     // ---- y-faces: rows 1..TY+1 solve the face below them -------------------------------
     F9 Fy;
-    if (w >= 1) {
+    if (w >= 1 && !halo_warp) {
       F9 L, R = face_lo<RECON>(mh, oy);
 #pragma unroll
       for (int i = 0; i < 9; ++i) L[i] = ybuf[((w - 1) * 9 + i) * 32 + lane];
@@ -326,7 +377,11 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     __syncthreads();
     if (row_own) {
 #pragma unroll
-      for (int i = 0; i < 9; ++i) dUxy[i] = dx_flux[i] + (Fy[i] - fybuf[(w * 9 + i) * 32 + lane]);
+      for (int i = 0; i < 9; ++i) {
+        const float dn = __shfl_down_sync(0xffffffffu, Fx[i], 1);
+        const float fxh = lane == TILE_X - 1 ? fxright[(w - 1) * 9 + i] : dn;
+        dUxy[i] = (Fx[i] - fxh) + (Fy[i] - fybuf[(w * 9 + i) * 32 + lane]);
+      }
     }
   }
   cp_async_wait_all();
@@ -358,7 +413,7 @@ __device__ __forceinline__ void cta_range(long long Q, long long* q0, long long*
 
 // One box: a persistent launch of one CTA per resident slot.
 template <int TY, int RECON, int RSOL, bool CT, bool COMP>
-__global__ void __launch_bounds__(32 * (TY + 2), 1) mhd_step_kernel(const __grid_constant__ StepArgs a) {
+__global__ void __launch_bounds__(step_threads<TY>(), 1) mhd_step_kernel(const __grid_constant__ StepArgs a) {
   extern __shared__ float smem[];
   long long q, qe;
   cta_range((long long)a.ntx * a.nty * a.nz, &q, &qe);
@@ -370,7 +425,7 @@ __global__ void __launch_bounds__(32 * (TY + 2), 1) mhd_step_kernel(const __grid
     march_column<TY, RECON, RSOL, CT, COMP>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax);
     q += z1 - z0;
   }
-  if (!CT && a.smax_bits != nullptr) flush_smax<32 * (TY + 2)>(smax, a.smax_bits);
+  if (!CT && a.smax_bits != nullptr) flush_smax<step_threads<TY>()>(smax, a.smax_bits);
 }
 
 // Many boxes in one launch: box b owns global indices [q0_b, q0_{b+1}) of the concatenated
@@ -381,7 +436,7 @@ struct BoxStep {
 };
 
 template <int TY, int RECON, int RSOL, bool CT, bool COMP>
-__global__ void __launch_bounds__(32 * (TY + 2), 1) mhd_batch_kernel(const BoxStep* __restrict__ boxes, int nbox,
+__global__ void __launch_bounds__(step_threads<TY>(), 1) mhd_batch_kernel(const BoxStep* __restrict__ boxes, int nbox,
                                                                        long long Q) {
   extern __shared__ float smem[];
   long long q, qe;
@@ -396,7 +451,7 @@ __global__ void __launch_bounds__(32 * (TY + 2), 1) mhd_batch_kernel(const BoxSt
   float smax = 0.0f;
   while (q < qe) {
     while (b + 1 < nbox && boxes[b + 1].q0 <= q) {
-      if (!CT && boxes[b].a.smax_bits != nullptr) flush_smax<32 * (TY + 2)>(smax, boxes[b].a.smax_bits);
+      if (!CT && boxes[b].a.smax_bits != nullptr) flush_smax<step_threads<TY>()>(smax, boxes[b].a.smax_bits);
       smax = 0.0f;
       ++b;
     }
@@ -408,7 +463,7 @@ __global__ void __launch_bounds__(32 * (TY + 2), 1) mhd_batch_kernel(const BoxSt
     march_column<TY, RECON, RSOL, CT, COMP>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax);
     q += z1 - z0;
   }
-  if (!CT && boxes[b].a.smax_bits != nullptr) flush_smax<32 * (TY + 2)>(smax, boxes[b].a.smax_bits);
+  if (!CT && boxes[b].a.smax_bits != nullptr) flush_smax<step_threads<TY>()>(smax, boxes[b].a.smax_bits);
 }
 
 }  // namespace pmf

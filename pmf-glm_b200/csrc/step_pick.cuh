@@ -44,7 +44,7 @@ StepKernel pick_rs(int rsol, bool ct, bool comp) {
 }
 template <int TY>
 StepKernelInfo info(int recon, int rsol, bool ct, bool comp) {
-  StepKernelInfo k{nullptr, StepSmem<TY>::BYTES, 32 * (TY + 2)};
+  StepKernelInfo k{nullptr, StepSmem<TY>::BYTES, step_threads<TY>()};
   switch (recon) {
     case RECON_PLM: k.fn = pick_rs<TY, RECON_PLM>(rsol, ct, comp); break;
     case RECON_PPM: k.fn = pick_rs<TY, RECON_PPM>(rsol, ct, comp); break;
