@@ -45,6 +45,24 @@ __device__ __forceinline__ F9 neg9(const F9& a) {
   return r;
 }
 
+// ---- packed FP32 pairs (sm_100 FFMA2 / FMUL2 / FADD2): two independent evaluations of the
+// same expression in one instruction, each lane rounded exactly as the scalar operation ----
+__device__ __forceinline__ float2 p2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 pb(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// a*b - c*d per lane
+__device__ __forceinline__ float2 msub2(float2 a, float2 b, float2 c, float2 d) {
+  return fma2(a, b, make_float2(-(c.x * d.x), -(c.y * d.y)));
+}
+struct P9 {
+  float2 v[9];
+  __device__ __forceinline__ float2& operator[](int i) { return v[i]; }
+  __device__ __forceinline__ const float2& operator[](int i) const { return v[i]; }
+};
+
 // conserved -> primitive with density and pressure floors (glm_physics.jl:11-18)
 __device__ __forceinline__ F9 cons2prim(const F9& c, float g, float smallr, float pfl) {
   float rho = fmaxf(c[0], smallr);
@@ -134,13 +152,23 @@ template <> struct Offsets<RECON_PPM> {
   __device__ __forceinline__ float l(int i) const { return dL[i]; }
 };
 
+// Half the MonCen slope, 0.5*moncen(dl, dr) of glm_physics.jl:47-53, with the scalings by
+// powers of two folded: 0.5*sgn*min(2*min|dl|,|dr|, |(dl+dr)/2|) = sgn*min(min(|dl|,|dr|),
+// |dl+dr|/4). Every rescaling is exact, so the result has the same bits.
+__device__ __forceinline__ float half_moncen(float dl, float dr) {
+  const float sum = dl + dr;
+  const float m = fminf(fminf(fabsf(dl), fabsf(dr)), 0.25f * fabsf(sum));
+  const float s = copysignf(m, sum);
+  return dl * dr <= 0.0f ? 0.0f : s;
+}
+
 template <int RECON>
 __device__ __forceinline__ Offsets<RECON> recon(const F9& mm, const F9& m0, const F9& mp) {
   Offsets<RECON> o;
 #pragma unroll
   for (int i = 0; i < 9; ++i) {
     if constexpr (RECON == RECON_PLM) {
-      o.dR[i] = 0.5f * moncen(m0[i] - mm[i], mp[i] - m0[i]);
+      o.dR[i] = half_moncen(m0[i] - mm[i], mp[i] - m0[i]);
     } else if constexpr (RECON == RECON_PLM_MINMOD) {
       o.dR[i] = 0.5f * minmod(m0[i] - mm[i], mp[i] - m0[i]);
     } else {
@@ -165,11 +193,48 @@ template <int RECON> __device__ __forceinline__ F9 face_hi(const F9& mh, const O
   return r;
 }
 
-// flux difference F(m0 + dR) - F(m0 + dL) along axis D (one term of the Hancock predictor)
+// x-normal flux of two primitive states at once (lane x and lane y), glm_physics.jl:28-34.
+__device__ __forceinline__ P9 phys_flux_x2(const P9& q, float g) {
+  const float2 rho = q[0], vx = q[1], vy = q[2], vz = q[3], p = q[4], bx = q[5], by = q[6], bz = q[7];
+  const float2 b2 = fma2(bz, bz, fma2(by, by, mul2(bx, bx)));
+  const float2 half = pb(0.5f);
+  const float2 ptot = fma2(half, b2, p);
+  const float2 v2 = fma2(vz, vz, fma2(vy, vy, mul2(vx, vx)));
+  const float ig = 1.0f / (g - 1.0f);
+  const float2 E = fma2(half, b2, fma2(mul2(half, rho), v2, mul2(p, pb(ig))));
+  const float2 vb = fma2(vz, bz, fma2(vy, by, mul2(vx, bx)));
+  const float2 m = mul2(rho, vx);
+  P9 f;
+  f[0] = m;
+  f[1] = sub2(fma2(m, vx, ptot), mul2(bx, bx));
+  f[2] = sub2(mul2(m, vy), mul2(bx, by));
+  f[3] = sub2(mul2(m, vz), mul2(bx, bz));
+  f[4] = sub2(mul2(add2(E, ptot), vx), mul2(bx, vb));
+  f[5] = pb(0.0f);
+  f[6] = sub2(mul2(vx, by), mul2(vy, bx));
+  f[7] = sub2(mul2(vx, bz), mul2(vz, bx));
+  f[8] = pb(0.0f);
+  return f;
+}
+
+// flux difference F(m0 + dR) - F(m0 + dL) along axis D (one term of the Hancock predictor,
+// glm_physics.jl:225-231); the two face states are evaluated as one packed pair
 template <int D, int RECON>
 __device__ __forceinline__ F9 hancock_term(const F9& m0, const Offsets<RECON>& o, float g) {
-  F9 p = face_hi<RECON>(m0, o), m = face_lo<RECON>(m0, o);
-  return sub9(dir_flux<D>(p, g), dir_flux<D>(m, g));
+  // global -> D-normal component order, as rot_to<D>
+  constexpr int perm[3][9] = {{0, 1, 2, 3, 4, 5, 6, 7, 8}, {0, 2, 3, 1, 4, 6, 7, 5, 8}, {0, 3, 1, 2, 4, 7, 5, 6, 8}};
+  P9 q;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const int j = perm[D][i];
+    q[i] = add2(pb(m0[j]), p2(o.dR[j], o.l(j)));
+  }
+  const P9 f = phys_flux_x2(q, g);
+  F9 d;
+  // back to the global order (rot_back<D>) while taking the difference of the two lanes
+#pragma unroll
+  for (int i = 0; i < 9; ++i) d[perm[D][i]] = f[i].x - f[i].y;
+  return d;
 }
 
 // ---- Riemann solvers in the face-normal frame (x-normal after rot_to) -----------------
@@ -198,81 +263,89 @@ __device__ __forceinline__ F9 hll_x(const F9& L, const F9& R, float g, float bn,
   f[8] = fpsi;
   return f;
 }
-// single-star transverse state (glm_physics.jl:255-263)
-__device__ __forceinline__ void hlld_star(float d, float u, float v, float w, float by, float bz, float S, float bn,
-                                          float SM, float& ov, float& ow, float& oby, float& obz) {
-  float denK = d * (S - u) * (S - SM) - bn * bn;
-  if (fabsf(denK) < 1e-12f) {
-    ov = v; ow = w; oby = by; obz = bz;
-  } else {
-    float fac = bn * (SM - u) / denK;
-    ov = v - by * fac;
-    ow = w - bz * fac;
-    oby = by * (d * (S - u) * (S - u) - bn * bn) / denK;
-    obz = bz * (d * (S - u) * (S - u) - bn * bn) / denK;
-  }
-}
-// HLLD, Miyoshi & Kusano 2005 (glm_physics.jl:264-307)
+// HLLD, Miyoshi & Kusano 2005 (glm_physics.jl:255-307). The left and right halves of the
+// solver are the same algebra on the two states, so they run as packed pairs (lane x = L,
+// lane y = R); the scalar parts are the wave speeds, the contact speed and the doubly-starred
+// state, which mix both sides.
 __device__ __forceinline__ F9 hlld_x(const F9& L, const F9& R, float g, float bn, float fbn, float fpsi) {
-  const float dL = L[0], uL = L[1], vL = L[2], wL = L[3], pL = L[4], byL = L[6], bzL = L[7];
-  const float dR = R[0], uR = R[1], vR = R[2], wR = R[3], pR = R[4], byR = R[6], bzR = R[7];
-  float b2L = bn * bn + byL * byL + bzL * bzL, b2R = bn * bn + byR * byR + bzR * bzR;
-  float ptL = pL + 0.5f * b2L, ptR = pR + 0.5f * b2R;
-  float EL = pL / (g - 1.0f) + 0.5f * dL * (uL * uL + vL * vL + wL * wL) + 0.5f * b2L;
-  float ER = pR / (g - 1.0f) + 0.5f * dR * (uR * uR + vR * vR + wR * wR) + 0.5f * b2R;
-  float cfL = fast_speed(L, g, bn), cfR = fast_speed(R, g, bn);
-  float SL = fminf(fminf(uL, uR) - fmaxf(cfL, cfR), 0.0f);
-  float SR = fmaxf(fmaxf(uL, uR) + fmaxf(cfL, cfR), 0.0f);
-  float den = (SR - uR) * dR - (SL - uL) * dL;
-  float SM = ((SR - uR) * dR * uR - (SL - uL) * dL * uL - ptR + ptL) / den;
-  float pts = ((SR - uR) * dR * ptL - (SL - uL) * dL * ptR + dL * dR * (SR - uR) * (SL - uL) * (uR - uL)) / den;
-  float dLs = fmaxf(dL * (SL - uL) / (SL - SM), 1e-12f), dRs = fmaxf(dR * (SR - uR) / (SR - SM), 1e-12f);
-  float sqdLs = sqrtf(dLs), sqdRs = sqrtf(dRs);
-  float SLs = SM - fabsf(bn) / sqdLs, SRs = SM + fabsf(bn) / sqdRs;
-  float vyLs, vzLs, byLs, bzLs, vyRs, vzRs, byRs, bzRs;
-  hlld_star(dL, uL, vL, wL, byL, bzL, SL, bn, SM, vyLs, vzLs, byLs, bzLs);
-  hlld_star(dR, uR, vR, wR, byR, bzR, SR, bn, SM, vyRs, vzRs, byRs, bzRs);
-  float vdotbL = uL * bn + vL * byL + wL * bzL, vdotbLs = SM * bn + vyLs * byLs + vzLs * bzLs;
-  float ELs = ((SL - uL) * EL - ptL * uL + pts * SM + bn * (vdotbL - vdotbLs)) / (SL - SM);
-  float vdotbR = uR * bn + vR * byR + wR * bzR, vdotbRs = SM * bn + vyRs * byRs + vzRs * bzRs;
-  float ERs = ((SR - uR) * ER - ptR * uR + pts * SM + bn * (vdotbR - vdotbRs)) / (SR - SM);
-  float sgn = bn >= 0.0f ? 1.0f : -1.0f;
-  float invsum = 1.0f / (sqdLs + sqdRs);
-  float vyss = (sqdLs * vyLs + sqdRs * vyRs + (byRs - byLs) * sgn) * invsum;
-  float vzss = (sqdLs * vzLs + sqdRs * vzRs + (bzRs - bzLs) * sgn) * invsum;
-  float byss = (sqdLs * byRs + sqdRs * byLs + sqdLs * sqdRs * (vyRs - vyLs) * sgn) * invsum;
-  float bzss = (sqdLs * bzRs + sqdRs * bzLs + sqdLs * sqdRs * (vzRs - vzLs) * sgn) * invsum;
-  float vdotbss = SM * bn + vyss * byss + vzss * bzss;
-  float ELss = ELs - sqdLs * (vdotbLs - vdotbss) * sgn;
-  float ERss = ERs + sqdRs * (vdotbRs - vdotbss) * sgn;
-  // Only the selected fan state is assembled: the four branches of glm_physics.jl:297-305.
+  const float2 d = p2(L[0], R[0]), u = p2(L[1], R[1]), v = p2(L[2], R[2]), w = p2(L[3], R[3]);
+  const float2 p = p2(L[4], R[4]), by = p2(L[6], R[6]), bz = p2(L[7], R[7]);
+  const float2 half = pb(0.5f);
+  const float bn2 = bn * bn;
+  const float2 b2 = fma2(bz, bz, fma2(by, by, pb(bn2)));
+  const float2 pt = fma2(half, b2, p);
+  const float ig = 1.0f / (g - 1.0f);
+  const float2 E = fma2(half, b2, fma2(mul2(half, d), fma2(w, w, fma2(v, v, mul2(u, u))), mul2(p, pb(ig))));
+  // fast speeds (glm_physics.jl:24-27) with the normal field bn
+  const float2 id = p2(1.0f / L[0], 1.0f / R[0]);
+  const float2 c2 = mul2(mul2(pb(g), p), id);
+  const float2 bb = mul2(b2, id);
+  const float2 d2 = mul2(half, add2(bb, c2));
+  const float2 disc = sub2(mul2(d2, d2), mul2(mul2(c2, pb(bn2)), id));
+  const float2 in = add2(d2, p2(sqrtf(fmaxf(disc.x, 0.0f)), sqrtf(fmaxf(disc.y, 0.0f))));
+  const float cfL = sqrtf(in.x), cfR = sqrtf(in.y);
+  const float cf = fmaxf(cfL, cfR);
+  const float SL = fminf(fminf(u.x, u.y) - cf, 0.0f);
+  const float SR = fmaxf(fmaxf(u.x, u.y) + cf, 0.0f);
+  const float2 S = p2(SL, SR);
+  const float2 Su = sub2(S, u);         // S - u per side
+  const float2 dSu = mul2(Su, d);       // d (S - u)
+  const float den = dSu.y - dSu.x;
+  const float2 dSuu = mul2(dSu, u);
+  const float SM = ((dSuu.y - dSuu.x) - pt.y + pt.x) / den;
+  const float pts = ((dSu.y * pt.x - dSu.x * pt.y) + d.x * d.y * Su.y * Su.x * (u.y - u.x)) / den;
+  const float2 SSM = sub2(S, pb(SM));   // S - SM per side
+  const float2 ds = mul2(dSu, p2(1.0f / SSM.x, 1.0f / SSM.y));
+  const float dLs = fmaxf(ds.x, 1e-12f), dRs = fmaxf(ds.y, 1e-12f);
+  const float2 dst = p2(dLs, dRs);
+  const float sqL = sqrtf(dLs), sqR = sqrtf(dRs);
+  const float abn = fabsf(bn);
+  const float SLs = SM - abn / sqL, SRs = SM + abn / sqR;
+  // single-starred transverse states of both sides (glm_physics.jl:255-263)
+  const float2 denK = fma2(dSu, SSM, pb(-bn2));
+  const float2 nK = fma2(dSu, Su, pb(-bn2));       // d (S - u)^2 - bn^2
+  const float2 iK = p2(1.0f / denK.x, 1.0f / denK.y);
+  const float2 fac = mul2(mul2(pb(bn), sub2(pb(SM), u)), iK);
+  const float2 rK = mul2(nK, iK);
+  const bool degL = fabsf(denK.x) < 1e-12f, degR = fabsf(denK.y) < 1e-12f;
+  float2 vs = sub2(v, mul2(by, fac)), ws = sub2(w, mul2(bz, fac));
+  float2 bys = mul2(by, rK), bzs = mul2(bz, rK);
+  if (degL) { vs.x = v.x; ws.x = w.x; bys.x = by.x; bzs.x = bz.x; }
+  if (degR) { vs.y = v.y; ws.y = w.y; bys.y = by.y; bzs.y = bz.y; }
+  const float2 vdb = fma2(w, bz, fma2(v, by, mul2(u, pb(bn))));
+  const float2 vdbs = fma2(ws, bzs, fma2(vs, bys, pb(SM * bn)));
+  // E* = ((S - u) E - pt u + pts SM + bn (v.b - v*.b*)) / (S - SM)
+  const float2 Enum = fma2(pb(bn), sub2(vdb, vdbs), add2(sub2(mul2(Su, E), mul2(pt, u)), pb(pts * SM)));
+  const float2 Es = mul2(Enum, p2(1.0f / SSM.x, 1.0f / SSM.y));
+  const float sgn = bn >= 0.0f ? 1.0f : -1.0f;
+  const float invsum = 1.0f / (sqL + sqR);
+  const float vyss = (sqL * vs.x + sqR * vs.y + (bys.y - bys.x) * sgn) * invsum;
+  const float vzss = (sqL * ws.x + sqR * ws.y + (bzs.y - bzs.x) * sgn) * invsum;
+  const float byss = (sqL * bys.y + sqR * bys.x + sqL * sqR * (vs.y - vs.x) * sgn) * invsum;
+  const float bzss = (sqL * bzs.y + sqR * bzs.x + sqL * sqR * (ws.y - ws.x) * sgn) * invsum;
+  const float vdbss = SM * bn + vyss * byss + vzss * bzss;
+  // E** = E* -+ sqrt(d*) (v*.b* - v**.b**) sgn
+  const float2 Ess = fma2(mul2(p2(-sqL, sqR), pb(sgn)), sub2(vdbs, pb(vdbss)), Es);
+  // only the selected fan state is assembled: the four branches of glm_physics.jl:297-305
   F9 f;
-  if (SLs >= 0.0f) {
-    F9 FL = phys_flux_x(F9{{dL, uL, vL, wL, pL, bn, byL, bzL, 0.0f}}, g);
-    const float UL[8] = {dL, dL * uL, dL * vL, dL * wL, EL, bn, byL, bzL};
-    const float ULs[8] = {dLs, dLs * SM, dLs * vyLs, dLs * vzLs, ELs, bn, byLs, bzLs};
+  const bool left = SM >= 0.0f;
+  const float dK = left ? d.x : d.y, uK = left ? u.x : u.y, vK = left ? v.x : v.y, wK = left ? w.x : w.y;
+  const float pK = left ? p.x : p.y, byK = left ? by.x : by.y, bzK = left ? bz.x : bz.y;
+  const float EK = left ? E.x : E.y, SK = left ? SL : SR, dKs = left ? dLs : dRs;
+  const float vKs = left ? vs.x : vs.y, wKs = left ? ws.x : ws.y, byKs = left ? bys.x : bys.y;
+  const float bzKs = left ? bzs.x : bzs.y, EKs = left ? Es.x : Es.y, EKss = left ? Ess.x : Ess.y;
+  const float SKs = left ? SLs : SRs;
+  const bool outer = left ? (SLs >= 0.0f) : (SRs < 0.0f);
+  const F9 FK = phys_flux_x(F9{{dK, uK, vK, wK, pK, bn, byK, bzK, 0.0f}}, g);
+  const float UK[8] = {dK, dK * uK, dK * vK, dK * wK, EK, bn, byK, bzK};
+  const float UKs[8] = {dKs, dKs * SM, dKs * vKs, dKs * wKs, EKs, bn, byKs, bzKs};
+  if (outer) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) f[i] = FL[i] + SL * (ULs[i] - UL[i]);
-  } else if (SM >= 0.0f) {
-    F9 FL = phys_flux_x(F9{{dL, uL, vL, wL, pL, bn, byL, bzL, 0.0f}}, g);
-    const float UL[8] = {dL, dL * uL, dL * vL, dL * wL, EL, bn, byL, bzL};
-    const float ULs[8] = {dLs, dLs * SM, dLs * vyLs, dLs * vzLs, ELs, bn, byLs, bzLs};
-    const float ULss[8] = {dLs, dLs * SM, dLs * vyss, dLs * vzss, ELss, bn, byss, bzss};
-#pragma unroll
-    for (int i = 0; i < 8; ++i) f[i] = FL[i] + SLs * ULss[i] - (SLs - SL) * ULs[i] - SL * UL[i];
-  } else if (SRs >= 0.0f) {
-    F9 FR = phys_flux_x(F9{{dR, uR, vR, wR, pR, bn, byR, bzR, 0.0f}}, g);
-    const float UR[8] = {dR, dR * uR, dR * vR, dR * wR, ER, bn, byR, bzR};
-    const float URs[8] = {dRs, dRs * SM, dRs * vyRs, dRs * vzRs, ERs, bn, byRs, bzRs};
-    const float URss[8] = {dRs, dRs * SM, dRs * vyss, dRs * vzss, ERss, bn, byss, bzss};
-#pragma unroll
-    for (int i = 0; i < 8; ++i) f[i] = FR[i] + SRs * URss[i] - (SRs - SR) * URs[i] - SR * UR[i];
+    for (int i = 0; i < 8; ++i) f[i] = FK[i] + SK * (UKs[i] - UK[i]);
   } else {
-    F9 FR = phys_flux_x(F9{{dR, uR, vR, wR, pR, bn, byR, bzR, 0.0f}}, g);
-    const float UR[8] = {dR, dR * uR, dR * vR, dR * wR, ER, bn, byR, bzR};
-    const float URs[8] = {dRs, dRs * SM, dRs * vyRs, dRs * vzRs, ERs, bn, byRs, bzRs};
+    const float UKss[8] = {dKs, dKs * SM, dKs * vyss, dKs * vzss, EKss, bn, byss, bzss};
 #pragma unroll
-    for (int i = 0; i < 8; ++i) f[i] = FR[i] + SR * (URs[i] - UR[i]);
+    for (int i = 0; i < 8; ++i) f[i] = FK[i] + SKs * UKss[i] - (SKs - SK) * UKs[i] - SK * UK[i];
   }
   f[5] = fbn;
   f[8] = fpsi;

@@ -31,7 +31,7 @@ constexpr int TILE_X = 32;  // owned columns per CTA: one warp lane per column
 constexpr int PLANE_W = 36; // primitive ring width: x0-2 .. x0+33
 
 // Threads per CTA: TY+2 row warps and the halo warp.
-template <int TY> constexpr int step_threads() { return 32 * (TY + 3); }
+template <int TY> __host__ __device__ constexpr int step_threads() { return 32 * (TY + 3); }
 
 // Number of CT workspace arrays written by the Godunov stage (reference CTState slots 4-15).
 constexpr int CT_NWORK = 12;
@@ -59,8 +59,11 @@ struct StepSmem {
   static constexpr int PRIM = 3 * 9 * PP;           // 3-plane primitive ring
   static constexpr int YB = (TY + 1) * 9 * 32;      // y-face states / fluxes
   static constexpr int XB = TY * 9;                 // one x-face state or flux per owned row
-  static constexpr int ZC = TY * 18 * 32;           // per owned thread: upper z state, lower z flux
-  static constexpr int FLOATS = STAGE + PRIM + 2 * YB + 3 * XB + ZC;
+  static constexpr int ZC = TY * 27 * 32;           // per owned thread: upper z state, lower z flux, x/y divergence
+  static constexpr int YL = (TY + 1) * 9 * 32;      // lower y state of rows 1..TY+1, parked
+  static constexpr int KE = (PP + 32 * (TY + 3) - 1) / (32 * (TY + 3));  // staged entries per thread
+  static constexpr int SI = 2 * KE * 32 * (TY + 3); // per thread: source (x, y) offset and flip bits
+  static constexpr int FLOATS = STAGE + PRIM + 2 * YB + 3 * XB + ZC + YL + SI;
   static constexpr size_t BYTES = sizeof(float) * FLOATS;
 };
 
@@ -86,7 +89,9 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   float* xleft = fybuf + S::YB;    // [row][9] upper x state of the left halo cell
   float* xright = xleft + S::XB;   // [row][9] upper x state of lane 31
   float* fxright = xright + S::XB; // [row][9] flux through the face above lane 31
-  float* zcarry = fxright + S::XB; // [row][18][32] upper z state and lower z flux of plane p-1
+  float* zcarry = fxright + S::XB; // [row][27][32] upper z state, lower z flux, x/y divergence of p-1
+  float* ylow = zcarry + S::ZC;    // [row-1][9][32] lower y state of rows 1..TY+1
+  int* sidx = reinterpret_cast<int*>(ylow + S::YL);  // [KE][2][NT] staging map of this segment
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5;
@@ -109,18 +114,33 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   const bool row_own = w >= 1 && w <= TY;
   const bool own = row_own && x < nx && y < ny;
 
-  // Source cell of staged-plane entry e (row r, column c) of logical plane zp, with BCs.
-  auto issue_plane = [&](int zp) {
-    float fz;
-    const int kz = bc_index(zp, nz, a.bc[2], &fz);
-    for (int e = tid; e < PP; e += NT) {
+  // Staging map of this column: for each staged entry e (row r, column c) this thread
+  // handles, the in-plane source offset iy*nx+ix under the x/y boundary rules and the
+  // reflecting-wall flips (bit 0: x, bit 1: y). It is the same for every plane, so it is
+  // built once per segment; per plane only the z index is resolved.
+#pragma unroll
+  for (int k = 0; k < S::KE; ++k) {
+    const int e = tid + k * NT;
+    if (e < PP) {
       const int r = e / PLANE_W, c = e - r * PLANE_W;
       float fx, fy;
       const int ix = bc_index(x0 + c - 2, nx, a.bc[0], &fx);
       const int iy = bc_index(y0 + r - 2, ny, a.bc[1], &fy);
-      const int gi = kz * nxy + iy * nx + ix;
+      sidx[(2 * k) * NT + tid] = iy * nx + ix;
+      sidx[(2 * k + 1) * NT + tid] = (fx < 0.0f ? 1 : 0) | (fy < 0.0f ? 2 : 0);
+    }
+  }
+  auto issue_plane = [&](int zp) {
+    float fz;
+    const int kz = bc_index(zp, nz, a.bc[2], &fz);
 #pragma unroll
-      for (int f = 0; f < 9; ++f) cp_async4(stage + f * PP + e, a.U[f] + gi);
+    for (int k = 0; k < S::KE; ++k) {
+      const int e = tid + k * NT;
+      if (e < PP) {
+        const int gi = kz * nxy + sidx[(2 * k) * NT + tid];
+#pragma unroll
+        for (int f = 0; f < 9; ++f) cp_async4(stage + f * PP + e, a.U[f] + gi);
+      }
     }
     cp_async_commit();
   };
@@ -128,20 +148,22 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   auto convert_plane = [&](int zp, float* dst) {
     float fz;
     bc_index(zp, nz, a.bc[2], &fz);
-    for (int e = tid; e < PP; e += NT) {
-      const int r = e / PLANE_W, c = e - r * PLANE_W;
-      float fx, fy;
-      bc_index(x0 + c - 2, nx, a.bc[0], &fx);
-      bc_index(y0 + r - 2, ny, a.bc[1], &fy);
-      F9 u;
 #pragma unroll
-      for (int f = 0; f < 9; ++f) u[f] = stage[f * PP + e];
-      u[1] *= fx; u[5] *= fx;
-      u[2] *= fy; u[6] *= fy;
-      u[3] *= fz; u[7] *= fz;
-      F9 q = cons2prim(u, g, P.smallr, P.pfl);
+    for (int k = 0; k < S::KE; ++k) {
+      const int e = tid + k * NT;
+      if (e < PP) {
+        const int fl = sidx[(2 * k + 1) * NT + tid];
+        const float fx = (fl & 1) ? -1.0f : 1.0f, fy = (fl & 2) ? -1.0f : 1.0f;
+        F9 u;
 #pragma unroll
-      for (int f = 0; f < 9; ++f) dst[f * PP + e] = q[f];
+        for (int f = 0; f < 9; ++f) u[f] = stage[f * PP + e];
+        u[1] *= fx; u[5] *= fx;
+        u[2] *= fy; u[6] *= fy;
+        u[3] *= fz; u[7] *= fz;
+        F9 q = cons2prim(u, g, P.smallr, P.pfl);
+#pragma unroll
+        for (int f = 0; f < 9; ++f) dst[f * PP + e] = q[f];
+      }
     }
   };
   auto slot = [&](int zp) { return prim + ((zp - z0 + 3) % 3) * (9 * PP); };
@@ -166,11 +188,11 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   __syncthreads();
   issue_plane(z0);
 
-  // Per-column carries across planes (owned rows only): the upper z-face state and the
-  // lower z-face flux of plane p-1 live in this thread's private slots of `zcarry`; the
-  // x/y divergence of plane p-1 stays in registers.
-  F9 dUxy;    // (Fxl - Fxh) + (Fyl - Fyh) of plane p-1
-  float* zc = zcarry + (row_own ? (w - 1) : 0) * 18 * 32 + lane;
+  // Per-column carries across planes (owned rows only), in this thread's private slots of
+  // `zcarry`: the upper z-face state (0..8) and the lower z-face flux (9..17) of plane p-1 and
+  // its x/y divergence ((Fxl - Fxh) + (Fyl - Fyh), 18..26). Parking them in shared memory
+  // keeps only the current solve's states in registers.
+  float* zc = zcarry + (row_own ? (w - 1) : 0) * 27 * 32 + lane;
   auto zc_store = [&](int off, const F9& v) {
 #pragma unroll
     for (int i = 0; i < 9; ++i) zc[(off + i) * 32] = v[i];
@@ -223,13 +245,11 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     }
     if (!CT && a.smax_bits != nullptr) smax = fmaxf(smax, cell_wavespeed(un, P));
   };
-  // Staggered normal field of this thread's cell's lower face along axis D (CT).
+  // Staggered normal field of this thread's cell's lower face along axis D (CT, periodic).
+  // x, y and pz are at most one period outside the box, so one conditional wrap suffices.
+  auto wrap1 = [](int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); };
   auto face_bn = [&](int D, int pz) {
-    float f0;
-    const int ix = bc_index(x, nx, BC_PERIODIC, &f0);
-    const int iy = bc_index(y, ny, BC_PERIODIC, &f0);
-    const int kz = bc_index(pz, nz, BC_PERIODIC, &f0);
-    return __ldg(a.face[D] + kz * nxy + iy * nx + ix);
+    return __ldg(a.face[D] + wrap1(pz, nz) * nxy + wrap1(y, ny) * nx + wrap1(x, nx));
   };
 
   for (int p = z0 - 1; p <= z1; ++p) {
@@ -279,24 +299,39 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       zc_store(0, face_hi<RECON>(mh, oz));
       continue;
     }
-    // y-halo row 0 and the owned rows publish their upper y state for the face above
-    if (mid && w <= TY) {  // row warps 0..TY (the halo warp is w = TY+2)
-      const F9 yR = face_hi<RECON>(mh, oy);
+    if (mid && !halo_warp) {
+      // upper y state for the row above (row warps 0..TY); lower y state parked (rows 1..TY+1)
+      if (w <= TY) {
+        const F9 yR = face_hi<RECON>(mh, oy);
 #pragma unroll
-      for (int i = 0; i < 9; ++i) ybuf[(w * 9 + i) * 32 + lane] = yR[i];
+        for (int i = 0; i < 9; ++i) ybuf[(w * 9 + i) * 32 + lane] = yR[i];
+      }
+      if (w >= 1) {
+        const F9 yL = face_lo<RECON>(mh, oy);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) ylow[((w - 1) * 9 + i) * 32 + lane] = yL[i];
+      }
+    }
+    // x-face states at the tile edges go through shared memory
+    if (mid && row_own && lane == TILE_X - 1) {
+      const F9 xR = face_hi<RECON>(mh, ox);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) xright[(w - 1) * 9 + i] = xR[i];
+    }
+    if (mid && halo_act && hside == 0) {
+      const F9 xR = face_hi<RECON>(mh, ox);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) xleft[hrow * 9 + i] = xR[i];
     }
     if (row_own) {
       // ---- z-face p-1/2: left = carried upper z state of p-1, right = lower z state of p --
-      F9 Fz;
-      {
-        F9 L = zc_load(0), R = face_lo<RECON>(mh, oz);
-        if constexpr (CT) {
-          const float bn = face_bn(2, p);
-          L[7] = bn; R[7] = bn;
-        }
-        Fz = riemann<2, RSOL, CT>(L, R, ch, P);
-      }
+      F9 L = zc_load(0), R = face_lo<RECON>(mh, oz);
       zc_store(0, face_hi<RECON>(mh, oz));
+      if constexpr (CT) {
+        const float bn = face_bn(2, p);
+        L[7] = bn; R[7] = bn;
+      }
+      const F9 Fz = riemann<2, RSOL, CT>(L, R, ch, P);
       if constexpr (CT) {
         if (own && mid) {
           a.work[2][cell_p] = Fz[0];
@@ -304,66 +339,59 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
           a.work[8][cell_p] = Fz[6];
         }
       }
-      if (p > z0 && own) update_cell(p - 1, dUxy, zc_load(9), Fz);
+      if (p > z0 && own) update_cell(p - 1, zc_load(18), zc_load(9), Fz);
       zc_store(9, Fz);
     }
     if (!mid) continue;  // p == z1: only the last z-face and update were needed
-
-    // ---- x-face states at the tile edges go through shared memory ----------------------
-    if (row_own && lane == TILE_X - 1) {
-      const F9 xR = face_hi<RECON>(mh, ox);
-#pragma unroll
-      for (int i = 0; i < 9; ++i) xright[(w - 1) * 9 + i] = xR[i];
-    }
-    if (halo_act && hside == 0) {
-      const F9 xR = face_hi<RECON>(mh, ox);
-#pragma unroll
-      for (int i = 0; i < 9; ++i) xleft[hrow * 9 + i] = xR[i];
-    }
     __syncthreads();
+
     // ---- x-faces: lane l of a row warp solves the face below column l (lane 0 against the
     // left halo cell); the halo warp's right-side lanes solve the face above lane 31. Both
     // go through this one call site, so a face shared by two tiles gets the same bits.
-    F9 xup;
-    {
-      const F9 xR = face_hi<RECON>(mh, ox);
-#pragma unroll
-      for (int i = 0; i < 9; ++i) xup[i] = __shfl_up_sync(0xffffffffu, xR[i], 1);
-    }
     F9 Fx;
-    if (row_own || (halo_act && hside == 1)) {
+    {
       F9 L, R = face_lo<RECON>(mh, ox);
+      {
+        const F9 xR = face_hi<RECON>(mh, ox);
 #pragma unroll
-      for (int i = 0; i < 9; ++i)
-        L[i] = halo_warp ? xright[hrow * 9 + i] : (lane == 0 ? xleft[(w - 1) * 9 + i] : xup[i]);
-      if constexpr (CT) {
-        const float bn = face_bn(0, p);
-        L[5] = bn; R[5] = bn;
+        for (int i = 0; i < 9; ++i) L[i] = __shfl_up_sync(0xffffffffu, xR[i], 1);
       }
-      Fx = riemann<0, RSOL, CT>(L, R, ch, P);
-      if (halo_warp) {
+      if (row_own || (halo_act && hside == 1)) {
 #pragma unroll
-        for (int i = 0; i < 9; ++i) fxright[hrow * 9 + i] = Fx[i];
-      }
-      if constexpr (CT) {
-        if (own) {
-          a.work[0][cell_p] = Fx[0];
-          a.work[3][cell_p] = Fx[6];
-          a.work[4][cell_p] = Fx[7];
+        for (int i = 0; i < 9; ++i)
+          if (halo_warp) L[i] = xright[hrow * 9 + i];
+          else if (lane == 0) L[i] = xleft[(w - 1) * 9 + i];
+        if constexpr (CT) {
+          const float bn = face_bn(0, p);
+          L[5] = bn; R[5] = bn;
+        }
+        Fx = riemann<0, RSOL, CT>(L, R, ch, P);
+        if (halo_warp) {
+#pragma unroll
+          for (int i = 0; i < 9; ++i) fxright[hrow * 9 + i] = Fx[i];
+        }
+        if constexpr (CT) {
+          if (own) {
+            a.work[0][cell_p] = Fx[0];
+            a.work[3][cell_p] = Fx[6];
+            a.work[4][cell_p] = Fx[7];
+          }
         }
       }
     }
-    // ---- y-faces: rows 1..TY+1 solve the face below them -------------------------------
-    F9 Fy;
+    // ---- y-faces: rows 1..TY+1 solve the face below them from two shared-memory states ---
     if (w >= 1 && !halo_warp) {
-      F9 L, R = face_lo<RECON>(mh, oy);
+      F9 L, R;
 #pragma unroll
-      for (int i = 0; i < 9; ++i) L[i] = ybuf[((w - 1) * 9 + i) * 32 + lane];
+      for (int i = 0; i < 9; ++i) {
+        L[i] = ybuf[((w - 1) * 9 + i) * 32 + lane];
+        R[i] = ylow[((w - 1) * 9 + i) * 32 + lane];
+      }
       if constexpr (CT) {
         const float bn = face_bn(1, p);
         L[6] = bn; R[6] = bn;
       }
-      Fy = riemann<1, RSOL, CT>(L, R, ch, P);
+      const F9 Fy = riemann<1, RSOL, CT>(L, R, ch, P);
 #pragma unroll
       for (int i = 0; i < 9; ++i) fybuf[((w - 1) * 9 + i) * 32 + lane] = Fy[i];
       if constexpr (CT) {
@@ -376,12 +404,14 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     }
     __syncthreads();
     if (row_own) {
+      F9 dxy;
 #pragma unroll
       for (int i = 0; i < 9; ++i) {
         const float dn = __shfl_down_sync(0xffffffffu, Fx[i], 1);
         const float fxh = lane == TILE_X - 1 ? fxright[(w - 1) * 9 + i] : dn;
-        dUxy[i] = (Fx[i] - fxh) + (Fy[i] - fybuf[(w * 9 + i) * 32 + lane]);
+        dxy[i] = (Fx[i] - fxh) + (fybuf[((w - 1) * 9 + i) * 32 + lane] - fybuf[(w * 9 + i) * 32 + lane]);
       }
+      zc_store(18, dxy);
     }
   }
   cp_async_wait_all();
