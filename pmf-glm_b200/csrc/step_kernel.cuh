@@ -264,6 +264,18 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     // the halo warp only works on owned planes
     if (halo_warp && !(p >= z0 && p < z1)) continue;
 
+    // CT: the staggered normal fields of this cell's three lower faces, fetched now so that
+    // their latency overlaps the Hancock step (x: all solving lanes; y: rows 1..TY+1; z:
+    // owned rows)
+    float bnx = 0.0f, bny = 0.0f, bnz = 0.0f;
+    if constexpr (CT) {
+      if (p >= z0 && p < z1) {
+        if (row_own || (halo_act && hside == 1)) bnx = face_bn(0, p);
+        if (w >= 1 && !halo_warp) bny = face_bn(1, p);
+      }
+      if (row_own) bnz = face_bn(2, p);
+    }
+
     // ---- Hancock half step of this thread's cell in plane p ------------------------------
     const float* pm = slot(p - 1);
     const float* p0 = slot(p);
@@ -328,8 +340,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       F9 L = zc_load(0), R = face_lo<RECON>(mh, oz);
       zc_store(0, face_hi<RECON>(mh, oz));
       if constexpr (CT) {
-        const float bn = face_bn(2, p);
-        L[7] = bn; R[7] = bn;
+        L[7] = bnz; R[7] = bnz;
       }
       const F9 Fz = riemann<2, RSOL, CT>(L, R, ch, P);
       if constexpr (CT) {
@@ -362,8 +373,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
           if (halo_warp) L[i] = xright[hrow * 9 + i];
           else if (lane == 0) L[i] = xleft[(w - 1) * 9 + i];
         if constexpr (CT) {
-          const float bn = face_bn(0, p);
-          L[5] = bn; R[5] = bn;
+          L[5] = bnx; R[5] = bnx;
         }
         Fx = riemann<0, RSOL, CT>(L, R, ch, P);
         if (halo_warp) {
@@ -388,8 +398,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
         R[i] = ylow[((w - 1) * 9 + i) * 32 + lane];
       }
       if constexpr (CT) {
-        const float bn = face_bn(1, p);
-        L[6] = bn; R[6] = bn;
+        L[6] = bny; R[6] = bny;
       }
       const F9 Fy = riemann<1, RSOL, CT>(L, R, ch, P);
 #pragma unroll
