@@ -84,7 +84,7 @@ int aux_blocks(const pmfmhd_ctx* c, long long nc) {
 // equal share of the (column, plane) space, but never less than `tz` planes).
 Tune default_tune(const pmfmhd_ctx*, const pmfmhd_grid* g) {
   Tune t;
-  t.ty = g->ny >= 13 ? 13 : (g->ny >= 8 ? 8 : 5);
+  t.ty = g->ny >= 8 ? 8 : 5;
   t.tz = 16;
   return t;
 }

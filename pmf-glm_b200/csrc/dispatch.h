@@ -15,8 +15,8 @@ struct StepKernelInfo {
 };
 
 // Rows per CTA that are instantiated (tile candidates for the autotuner).
-constexpr int kTileRows[] = {5, 8, 13};
-constexpr int kNumTileRows = 3;
+constexpr int kTileRows[] = {5, 8, 10, 13};
+constexpr int kNumTileRows = 4;
 
 StepKernelInfo step_kernel_info(int ty, int recon, int rsol, bool ct, bool comp);
 // The many-box form of the same kernel (same shared memory and block size).

@@ -56,13 +56,14 @@ struct StepSmem {
   static constexpr int PH = TY + 4;                 // rows y0-2 .. y0+TY+1
   static constexpr int PP = PLANE_W * PH;           // cells per staged plane
   static constexpr int STAGE = 9 * PP;              // raw conserved plane
-  static constexpr int PRIM = 3 * 9 * PP;           // 3-plane primitive ring
+  static constexpr int PRIM = 4 * 9 * PP;           // 4-plane primitive ring
   static constexpr int YB = (TY + 1) * 9 * 32;      // y-face states / fluxes
   static constexpr int XB = TY * 9;                 // one x-face state or flux per owned row
   static constexpr int ZC = TY * 27 * 32;           // per owned thread: upper z state, lower z flux, x/y divergence
   static constexpr int YL = (TY + 1) * 9 * 32;      // lower y state of rows 1..TY+1, parked
-  static constexpr int KE = (PP + 32 * (TY + 3) - 1) / (32 * (TY + 3));  // staged entries per thread
-  static constexpr int SI = 2 * KE * 32 * (TY + 3); // per thread: source (x, y) offset and flip bits
+  static constexpr int NL = 96;                     // loader threads: warps 0, TY+1 and the halo warp
+  static constexpr int KL = (PP + NL - 1) / NL;     // staged entries per loader thread
+  static constexpr int SI = 2 * KL * NL;            // per loader: source (x, y) offset and flip bits
   static constexpr int FLOATS = STAGE + PRIM + 2 * YB + 3 * XB + ZC + YL + SI;
   static constexpr size_t BYTES = sizeof(float) * FLOATS;
 };
@@ -91,7 +92,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   float* fxright = xright + S::XB; // [row][9] flux through the face above lane 31
   float* zcarry = fxright + S::XB; // [row][27][32] upper z state, lower z flux, x/y divergence of p-1
   float* ylow = zcarry + S::ZC;    // [row-1][9][32] lower y state of rows 1..TY+1
-  int* sidx = reinterpret_cast<int*>(ylow + S::YL);  // [KE][2][NT] staging map of this segment
+  int* sidx = reinterpret_cast<int*>(ylow + S::YL);  // [KL][2][NL] staging map of this segment
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5;
@@ -114,45 +115,52 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   const bool row_own = w >= 1 && w <= TY;
   const bool own = row_own && x < nx && y < ny;
 
-  // Staging map of this column: for each staged entry e (row r, column c) this thread
-  // handles, the in-plane source offset iy*nx+ix under the x/y boundary rules and the
-  // reflecting-wall flips (bit 0: x, bit 1: y). It is the same for every plane, so it is
-  // built once per segment; per plane only the z index is resolved.
+  // Staging is done by the three "loader" warps (the two y-halo rows and the halo warp),
+  // which have the least solving to do: they prefetch plane p+3 by cp.async and convert
+  // plane p+2 into the primitive ring while the owned rows solve plane p.
+  const bool loader = w == 0 || w >= TY + 1;
+  const int lt = w == 0 ? lane : (w == TY + 1 ? 32 + lane : 64 + lane);
+  // Staging map of this column: for each staged entry e (row r, column c) a loader handles,
+  // the in-plane source offset iy*nx+ix under the x/y boundary rules and the reflecting-wall
+  // flips (bit 0: x, bit 1: y). It is the same for every plane, so it is built once per
+  // segment; per plane only the z index is resolved.
+  if (loader) {
 #pragma unroll
-  for (int k = 0; k < S::KE; ++k) {
-    const int e = tid + k * NT;
-    if (e < PP) {
-      const int r = e / PLANE_W, c = e - r * PLANE_W;
-      float fx, fy;
-      const int ix = bc_index(x0 + c - 2, nx, a.bc[0], &fx);
-      const int iy = bc_index(y0 + r - 2, ny, a.bc[1], &fy);
-      sidx[(2 * k) * NT + tid] = iy * nx + ix;
-      sidx[(2 * k + 1) * NT + tid] = (fx < 0.0f ? 1 : 0) | (fy < 0.0f ? 2 : 0);
+    for (int k = 0; k < S::KL; ++k) {
+      const int e = lt + k * S::NL;
+      if (e < PP) {
+        const int r = e / PLANE_W, c = e - r * PLANE_W;
+        float fx, fy;
+        const int ix = bc_index(x0 + c - 2, nx, a.bc[0], &fx);
+        const int iy = bc_index(y0 + r - 2, ny, a.bc[1], &fy);
+        sidx[(2 * k) * S::NL + lt] = iy * nx + ix;
+        sidx[(2 * k + 1) * S::NL + lt] = (fx < 0.0f ? 1 : 0) | (fy < 0.0f ? 2 : 0);
+      }
     }
   }
-  auto issue_plane = [&](int zp) {
+  auto issue_plane = [&](int zp) {  // loaders only
     float fz;
     const int kz = bc_index(zp, nz, a.bc[2], &fz);
 #pragma unroll
-    for (int k = 0; k < S::KE; ++k) {
-      const int e = tid + k * NT;
+    for (int k = 0; k < S::KL; ++k) {
+      const int e = lt + k * S::NL;
       if (e < PP) {
-        const int gi = kz * nxy + sidx[(2 * k) * NT + tid];
+        const int gi = kz * nxy + sidx[(2 * k) * S::NL + lt];
 #pragma unroll
         for (int f = 0; f < 9; ++f) cp_async4(stage + f * PP + e, a.U[f] + gi);
       }
     }
     cp_async_commit();
   };
-  // Raw conserved -> primitive (reflecting walls flip the normal components first).
+  // Raw conserved -> primitive (reflecting walls flip the normal components first); loaders.
   auto convert_plane = [&](int zp, float* dst) {
     float fz;
     bc_index(zp, nz, a.bc[2], &fz);
 #pragma unroll
-    for (int k = 0; k < S::KE; ++k) {
-      const int e = tid + k * NT;
+    for (int k = 0; k < S::KL; ++k) {
+      const int e = lt + k * S::NL;
       if (e < PP) {
-        const int fl = sidx[(2 * k + 1) * NT + tid];
+        const int fl = sidx[(2 * k + 1) * S::NL + lt];
         const float fx = (fl & 1) ? -1.0f : 1.0f, fy = (fl & 2) ? -1.0f : 1.0f;
         F9 u;
 #pragma unroll
@@ -166,7 +174,9 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       }
     }
   };
-  auto slot = [&](int zp) { return prim + ((zp - z0 + 3) % 3) * (9 * PP); };
+  // barrier among the loader warps only (named barrier 1)
+  auto loader_sync = [&]() { asm volatile("bar.sync 1, %0;\n" ::"r"(S::NL) : "memory"); };
+  auto slot = [&](int zp) { return prim + ((zp - z0 + 4) & 3) * (9 * PP); };
   auto ld9 = [&](const float* pl, int r, int c) {
     F9 q;
 #pragma unroll
@@ -174,19 +184,18 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     return q;
   };
 
-  // Prologue: primitives of planes z0-2 and z0-1, plane z0 in flight.
-  __syncthreads();
-  issue_plane(z0 - 2);
-  cp_async_wait_all();
-  __syncthreads();
-  convert_plane(z0 - 2, slot(z0 - 2));
-  __syncthreads();
-  issue_plane(z0 - 1);
-  cp_async_wait_all();
-  __syncthreads();
-  convert_plane(z0 - 1, slot(z0 - 1));
-  __syncthreads();
-  issue_plane(z0);
+  // Prologue: primitives of planes z0-2, z0-1 and z0, plane z0+1 in flight.
+  __syncthreads();  // the previous segment may still be reading shared memory
+  if (loader) {
+    for (int zp = z0 - 2; zp <= z0; ++zp) {
+      issue_plane(zp);
+      cp_async_wait_all();
+      loader_sync();
+      convert_plane(zp, slot(zp));
+      loader_sync();
+    }
+    if (z0 + 1 <= z1 + 1) issue_plane(z0 + 1);
+  }
 
   // Per-column carries across planes (owned rows only), in this thread's private slots of
   // `zcarry`: the upper z-face state (0..8) and the lower z-face flux (9..17) of plane p-1 and
@@ -253,21 +262,19 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   };
 
   for (int p = z0 - 1; p <= z1; ++p) {
-    cp_async_wait_all();
-    __syncthreads();
-    convert_plane(p + 1, slot(p + 1));
-    __syncthreads();
-    if (p + 2 <= z1 + 1) issue_plane(p + 2);
-
-    // plane z0-1 only feeds the lower z-face of the chunk: only the owned rows need it
-    if (p == z0 - 1 && !row_own) continue;
-    // the halo warp only works on owned planes
-    if (halo_warp && !(p >= z0 && p < z1)) continue;
+    __syncthreads();  // plane p+1 (converted during the previous pass) is in the ring
+    const bool mid = p >= z0 && p < z1;  // an owned plane of this chunk
+    const int cell_p = (mid && x < nx && y < ny) ? (p * nxy + y * nx + x) : 0;
+    // this thread's Hancock state and face offsets of plane p, and (CT) its lower-face fields
+    F9 mh;
+    Offsets<RECON> ox, oy, oz;
+    float bnx = 0.0f, bny = 0.0f, bnz = 0.0f;
+    // planes z0-1 and z1 only feed the chunk's end z-faces: only the owned rows work on them
+    if (mid || row_own) {
 
     // CT: the staggered normal fields of this cell's three lower faces, fetched now so that
     // their latency overlaps the Hancock step (x: all solving lanes; y: rows 1..TY+1; z:
     // owned rows)
-    float bnx = 0.0f, bny = 0.0f, bnz = 0.0f;
     if constexpr (CT) {
       if (p >= z0 && p < z1) {
         if (row_own || (halo_act && hside == 1)) bnx = face_bn(0, p);
@@ -281,10 +288,9 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     const float* p0 = slot(p);
     const float* pp = slot(p + 1);
     const F9 m0 = ld9(p0, r0, c0);
-    const Offsets<RECON> ox = recon<RECON>(ld9(p0, r0, c0 - 1), m0, ld9(p0, r0, c0 + 1));
-    const Offsets<RECON> oy = recon<RECON>(ld9(p0, r0 - 1, c0), m0, ld9(p0, r0 + 1, c0));
-    const Offsets<RECON> oz = recon<RECON>(ld9(pm, r0, c0), m0, ld9(pp, r0, c0));
-    F9 mh;
+    ox = recon<RECON>(ld9(p0, r0, c0 - 1), m0, ld9(p0, r0, c0 + 1));
+    oy = recon<RECON>(ld9(p0, r0 - 1, c0), m0, ld9(p0, r0 + 1, c0));
+    oz = recon<RECON>(ld9(pm, r0, c0), m0, ld9(pp, r0, c0));
     {
       const F9 u0 = prim2cons(m0, g);
       F9 acc = hancock_term<0, RECON>(m0, ox, g);
@@ -296,8 +302,6 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       for (int i = 0; i < 9; ++i) uh[i] = u0[i] - h * acc[i];
       mh = cons2prim(uh, g, P.smallr, P.pfl);
     }
-    const bool mid = p >= z0 && p < z1;  // an owned plane of this chunk
-    const int cell_p = (mid && x < nx && y < ny) ? (p * nxy + y * nx + x) : 0;
     if constexpr (CT) {
       // cell-centred reference EMF -v x B: v of the predicted state, B at the start of the
       // step (integrator_ref.jl:133-138)
@@ -309,8 +313,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     }
     if (p == z0 - 1) {
       zc_store(0, face_hi<RECON>(mh, oz));
-      continue;
-    }
+    } else {
     if (mid && !halo_warp) {
       // upper y state for the row above (row warps 0..TY); lower y state parked (rows 1..TY+1)
       if (w <= TY) {
@@ -353,7 +356,17 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       if (p > z0 && own) update_cell(p - 1, zc_load(18), zc_load(9), Fz);
       zc_store(9, Fz);
     }
-    if (!mid) continue;  // p == z1: only the last z-face and update were needed
+    }  // p > z0 - 1
+    }  // mid || row_own
+    // ---- loaders: convert plane p+2 (its ring slot last held p-2) and prefetch p+3 -----------
+    if (loader && p + 2 <= z1 + 1) {
+      cp_async_wait_all();
+      loader_sync();
+      convert_plane(p + 2, slot(p + 2));
+      loader_sync();
+      if (p + 3 <= z1 + 1) issue_plane(p + 3);
+    }
+    if (!mid) continue;  // p == z0-1 or z1: only the chunk's end z-faces and update were needed
     __syncthreads();
 
     // ---- x-faces: lane l of a row warp solves the face below column l (lane 0 against the

@@ -1,0 +1,11 @@
+// Step-kernel instantiations for CTAs of 10 owned rows.
+#include "step_pick.cuh"
+
+namespace pmf {
+StepKernelInfo step_kernel_info_ty10(int recon, int rsol, bool ct, bool comp) {
+  return detail::info<10>(recon, rsol, ct, comp);
+}
+BatchKernel batch_kernel_ty10(int recon, int rsol, bool ct, bool comp) {
+  return detail::batch<10>(recon, rsol, ct, comp);
+}
+}  // namespace pmf
