@@ -180,6 +180,12 @@ int pmfmhd_batch_destroy(pmfmhd_batch* b);
 int pmfmhd_autotune(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], int mhd_solver,
                     int compensated, void* stream);
 
+/* Device status of the steps enqueued on this context since the last clearing call:
+ * PMFMHD_ETIMEOUT if a step kernel's bounded wait for a TMA plane load gave up (that step's
+ * result is invalid; staging fell back to per-element copies), else PMFMHD_OK. clear != 0
+ * resets the status. Blocking. */
+int pmfmhd_status(pmfmhd_ctx* ctx, int clear, void* stream);
+
 /* Pin (or query) the tile used for this grid/solver/mode on this context: `rows` owned rows
  * per CTA (an instantiated height: 5, 8, 10 or 13) and `planes` z-planes per CTA chunk. */
 int pmfmhd_set_tile(pmfmhd_ctx* ctx, const pmfmhd_grid* g, int mhd_solver, int compensated, int rows, int planes);

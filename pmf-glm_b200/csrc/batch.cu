@@ -269,6 +269,8 @@ int pmfmhd_batch_create(pmfmhd_ctx* c, const pmfmhd_box* boxes, int nbox, pmfmhd
         a.P = phys_of(&x.grid);
         a.smax_bits = g.ct ? nullptr : b->d_smax + i;
         a.dscal = b->d_dscal + 4 * i;
+        a.status = c->d_status;
+        a.use_tma = field_maps(c, &x.grid, a.U, g.ty, a.tmap) ? 1 : 0;
         d.q0 = q;
         desc[p].push_back(d);
       }

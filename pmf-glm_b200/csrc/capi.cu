@@ -1,6 +1,7 @@
 // C ABI of libpmfmhd.so: argument checks, tile selection, launches, CUDA-graph replay of
 // fixed-dt step sequences, and the FP64 diagnostics. See include/pmfmhd.h.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cmath>
 #include <cstring>
@@ -96,6 +97,49 @@ Tune tune_for(pmfmhd_ctx* c, const pmfmhd_grid* g, bool ct, bool comp) {
   return default_tune(c, g);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link to libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+bool field_maps(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], int ty, CUtensorMap out[9]) {
+  auto enc = encode_fn();
+  if (enc == nullptr || g->nx % 4 != 0 || g->nx < PLANE_W || g->ny < ty + 4) return false;
+  for (int f = 0; f < 9; ++f)
+    if (reinterpret_cast<uintptr_t>(U[f]) % 16 != 0) return false;
+  std::lock_guard<std::mutex> lk(c->mu);
+  for (int f = 0; f < 9; ++f) {
+    const MapKey key{U[f], g->nx, g->ny, g->nz, ty};
+    auto it = c->maps.find(key);
+    if (it != c->maps.end()) {
+      out[f] = it->second;
+      continue;
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)g->nx, (cuuint64_t)g->ny, (cuuint64_t)g->nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)g->nx * 4, (cuuint64_t)g->nx * g->ny * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)PLANE_W, (cuuint32_t)(ty + 4), 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUtensorMap m;
+    if (enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(U[f]), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+    if (c->maps.size() > 4096) c->maps.clear();
+    c->maps[key] = m;
+    out[f] = m;
+  }
+  return true;
+}
+
 // Resident CTAs per SM of a step kernel (cached per kernel).
 int occupancy_of(const StepKernelInfo& k) {
   static std::mutex mu;
@@ -113,7 +157,7 @@ int occupancy_of(const StepKernelInfo& k) {
   return occ;
 }
 
-int launch_step(const pmfmhd_ctx* c, const pmfmhd_grid* g, StepArgs& a, Tune t, bool ct, bool comp,
+int launch_step(pmfmhd_ctx* c, const pmfmhd_grid* g, StepArgs& a, Tune t, bool ct, bool comp,
                 cudaStream_t s) {
   StepKernelInfo k = step_kernel_info(t.ty, g->recon, g->riemann, ct, comp);
   if (k.fn == nullptr) return PMFMHD_EUNSUPPORTED;
@@ -123,6 +167,8 @@ int launch_step(const pmfmhd_ctx* c, const pmfmhd_grid* g, StepArgs& a, Tune t, 
   a.ntx = (g->nx + TILE_X - 1) / TILE_X;
   a.nty = (g->ny + t.ty - 1) / t.ty;
   a.P = phys_of(g);
+  a.status = c->d_status;
+  a.use_tma = field_maps(c, g, a.U, t.ty, a.tmap) ? 1 : 0;
   const long long Q = (long long)a.ntx * a.nty * g->nz;
   const long long slots = (long long)c->sms * occ;
   const long long by_work = std::max<long long>(1, (Q + t.tz - 1) / std::max(1, t.tz));
@@ -218,12 +264,14 @@ int pmfmhd_create(int device, pmfmhd_ctx** out) {
   if (cudaMalloc(&c->d_smax, 256) != cudaSuccess || cudaMalloc(&c->d_u64, 256) != cudaSuccess ||
       cudaMalloc(&c->d_partial, sizeof(double) * 8 * kTotBlocksMax) != cudaSuccess ||
       cudaMalloc(&c->d_tot, sizeof(double) * 8) != cudaSuccess || cudaMallocHost(&c->h_pin, 256) != cudaSuccess ||
+      cudaMalloc(&c->d_status, sizeof(unsigned int)) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking) != cudaSuccess) {
     last_cuda_error() = cudaGetErrorString(cudaGetLastError());
     pmfmhd_destroy(c);
     return PMFMHD_ENOMEM;
   }
   PMF_CK(cudaMemset(c->d_smax, 0, 256));
+  PMF_CK(cudaMemset(c->d_status, 0, sizeof(unsigned int)));
   *out = c;
   return PMFMHD_OK;
 }
@@ -237,6 +285,7 @@ int pmfmhd_destroy(pmfmhd_ctx* c) {
   cudaFree(c->d_u64);
   cudaFree(c->d_partial);
   cudaFree(c->d_tot);
+  cudaFree(c->d_status);
   cudaFreeHost(c->h_pin);
   delete c;
   return PMFMHD_OK;
@@ -507,6 +556,17 @@ int pmfmhd_autotune(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9]
     c->tune[TuneKey{g->nx, g->ny, g->nz, ct, comp, g->recon, g->riemann}] = best;
   }
   return result;
+}
+
+int pmfmhd_status(pmfmhd_ctx* c, int clear, void* stream) {
+  if (c == nullptr) return PMFMHD_EINVAL;
+  cudaStream_t s = as_stream(stream);
+  PMF_CK(cudaMemcpyAsync(c->h_pin, c->d_status, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+  PMF_CK(cudaStreamSynchronize(s));
+  unsigned int bits;
+  std::memcpy(&bits, c->h_pin, sizeof(bits));
+  if (clear) PMF_CK(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned int), s));
+  return bits & 1u ? PMFMHD_ETIMEOUT : PMFMHD_OK;
 }
 
 int pmfmhd_set_tile(pmfmhd_ctx* c, const pmfmhd_grid* g, int mhd_solver, int compensated, int rows, int planes) {

@@ -8,6 +8,8 @@
 #include <tuple>
 #include <vector>
 
+#include <cuda.h>
+
 #include "../../include/pmfmhd.h"
 #include "dispatch.h"
 #include "physics.cuh"
@@ -42,6 +44,14 @@ struct GraphEntry {
   cudaGraphExec_t exec;
 };
 
+struct MapKey {
+  const void* ptr;
+  int nx, ny, nz, ty;
+  bool operator<(const MapKey& o) const {
+    return std::tie(ptr, nx, ny, nz, ty) < std::tie(o.ptr, o.nx, o.ny, o.nz, o.ty);
+  }
+};
+
 int check_grid(const pmfmhd_grid* g);
 bool all_periodic(const pmfmhd_grid* g);
 Phys phys_of(const pmfmhd_grid* g);
@@ -62,12 +72,17 @@ struct pmfmhd_ctx {
   cudaStream_t cap = nullptr;               // stream used to record graphs
   std::map<pmf::host::TuneKey, pmf::host::Tune> tune;
   std::vector<pmf::host::GraphEntry> graphs;
+  std::map<pmf::host::MapKey, CUtensorMap> maps;  // TMA descriptors of field arrays
+  unsigned int* d_status = nullptr;                // device status bits of the step kernels
   std::mutex mu;
 };
 
 namespace pmf {
 namespace host {
 Tune tune_for(pmfmhd_ctx* c, const pmfmhd_grid* g, bool ct, bool comp);
+// Tensor maps for the nine fields U (box PLANE_W x (ty+4) x 1); false if TMA cannot be used
+// for this grid (x extent not a multiple of 4, unaligned pointers, box larger than the grid).
+bool field_maps(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], int ty, CUtensorMap out[9]);
 int aux_blocks(const pmfmhd_ctx* c, long long nc);
 }  // namespace host
 }  // namespace pmf

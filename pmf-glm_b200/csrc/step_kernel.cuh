@@ -23,12 +23,15 @@
 // state of the one-cell halo ring and the halo rows' y-faces.
 // The new state's max signal speed (timestep.jl:4-14) is reduced in the same pass.
 #pragma once
+#include <cuda.h>  // CUtensorMap (the tiled-tensor descriptor the TMA loads read)
+
 #include "physics.cuh"
 
 namespace pmf {
 
 constexpr int TILE_X = 32;  // owned columns per CTA: one warp lane per column
-constexpr int PLANE_W = 36; // primitive ring width: x0-2 .. x0+33
+constexpr int PLANE_W = 40; // staged plane width: x0-4 .. x0+35 (16-byte aligned rows for TMA)
+constexpr int PLANE_X0 = 4; // column of x0 in the staged plane
 
 // Threads per CTA: TY+2 row warps and the halo warp.
 template <int TY> __host__ __device__ constexpr int step_threads() { return 32 * (TY + 3); }
@@ -49,12 +52,16 @@ struct StepArgs {
   Phys P;
   unsigned int* smax_bits;  // fused CFL reduction target (bits of a non-negative float), or null
   const float* dscal;       // if non-null: device {dtdx, ch, decay} overriding the values above
+  unsigned int* status;     // device status bits (1: a bounded wait for a TMA load gave up), or null
+  int use_tma;              // the tensor maps below describe U (fields with nx % 4 == 0)
+  CUtensorMap tmap[9];      // per field: 3-D (x, y, z) FP32 map, box (PLANE_W, TY+4, 1)
 };
 
 template <int TY>
 struct StepSmem {
   static constexpr int PH = TY + 4;                 // rows y0-2 .. y0+TY+1
-  static constexpr int PP = PLANE_W * PH;           // cells per staged plane
+  static constexpr int PW = PLANE_W * PH;           // cells per staged plane
+  static constexpr int PP = (PW + 31) / 32 * 32;    // field stride: 128-byte aligned for TMA
   static constexpr int STAGE = 9 * PP;              // raw conserved plane
   static constexpr int PRIM = 4 * 9 * PP;           // 4-plane primitive ring
   static constexpr int YB = (TY + 1) * 9 * 32;      // y-face states / fluxes
@@ -62,7 +69,7 @@ struct StepSmem {
   static constexpr int ZC = TY * 27 * 32;           // per owned thread: upper z state, lower z flux, x/y divergence
   static constexpr int YL = (TY + 1) * 9 * 32;      // lower y state of rows 1..TY+1, parked
   static constexpr int NL = 96;                     // loader threads: warps 0, TY+1 and the halo warp
-  static constexpr int KL = (PP + NL - 1) / NL;     // staged entries per loader thread
+  static constexpr int KL = (PW + NL - 1) / NL;     // staged entries per loader thread
   static constexpr int SI = 2 * KL * NL;            // per loader: source (x, y) offset and flip bits
   static constexpr int FLOATS = STAGE + PRIM + 2 * YB + 3 * XB + ZC + YL + SI;
   static constexpr size_t BYTES = sizeof(float) * FLOATS;
@@ -79,7 +86,8 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Every thread of the CTA calls it; `smax` accumulates the new state's max signal speed.
 template <int TY, int RECON, int RSOL, bool CT, bool COMP>
 __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, int z0, int z1, float* smem,
-                                             float& smax) {
+                                             float& smax, unsigned long long* tma_bar, unsigned& tma_phase,
+                                             int* tma_off) {
   using S = StepSmem<TY>;
   constexpr int NT = step_threads<TY>();
   constexpr int PP = S::PP;
@@ -128,29 +136,79 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
 #pragma unroll
     for (int k = 0; k < S::KL; ++k) {
       const int e = lt + k * S::NL;
-      if (e < PP) {
+      if (e < S::PW) {
         const int r = e / PLANE_W, c = e - r * PLANE_W;
         float fx, fy;
-        const int ix = bc_index(x0 + c - 2, nx, a.bc[0], &fx);
+        const int ix = bc_index(x0 + c - PLANE_X0, nx, a.bc[0], &fx);
         const int iy = bc_index(y0 + r - 2, ny, a.bc[1], &fy);
         sidx[(2 * k) * S::NL + lt] = iy * nx + ix;
         sidx[(2 * k + 1) * S::NL + lt] = (fx < 0.0f ? 1 : 0) | (fy < 0.0f ? 2 : 0);
       }
     }
   }
+  // A plane whose staged box lies inside the grid comes in by TMA: one loader thread issues
+  // nine tiled bulk-tensor loads (no multicast) that complete on an mbarrier. Other planes
+  // (periodic wrap, outflow or reflecting ghosts) come in by per-element cp.async through the
+  // staging map.
+  const bool tma_cols = a.use_tma && (__cvta_generic_to_shared(stage) & 127) == 0 && x0 - PLANE_X0 >= 0 &&
+                        x0 - PLANE_X0 + PLANE_W <= nx && y0 - 2 >= 0 && y0 + TY + 2 <= ny;
+  bool pending_tma = false;  // the plane in flight came by TMA
+  const unsigned bar_addr = (unsigned)__cvta_generic_to_shared(tma_bar);
   auto issue_plane = [&](int zp) {  // loaders only
+    pending_tma = tma_cols && zp >= 0 && zp < nz && *tma_off == 0;
+    if (pending_tma) {
+      if (lt == 0) {
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar_addr),
+                     "r"((unsigned)(9 * S::PW * sizeof(float)))
+                     : "memory");
+#pragma unroll
+        for (int f = 0; f < 9; ++f) {
+          const unsigned dst = (unsigned)__cvta_generic_to_shared(stage + f * PP);
+          asm volatile(
+              "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+              "[%5];\n" ::"r"(dst),
+              "l"(reinterpret_cast<unsigned long long>(&a.tmap[f])), "r"(x0 - PLANE_X0), "r"(y0 - 2), "r"(zp),
+              "r"(bar_addr)
+              : "memory");
+        }
+      }
+      return;
+    }
     float fz;
     const int kz = bc_index(zp, nz, a.bc[2], &fz);
 #pragma unroll
     for (int k = 0; k < S::KL; ++k) {
       const int e = lt + k * S::NL;
-      if (e < PP) {
+      if (e < S::PW) {
         const int gi = kz * nxy + sidx[(2 * k) * S::NL + lt];
 #pragma unroll
         for (int f = 0; f < 9; ++f) cp_async4(stage + f * PP + e, a.U[f] + gi);
       }
     }
     cp_async_commit();
+  };
+  // Wait for the plane in flight (loaders only). A TMA wait is bounded: if the load never
+  // lands, the status flag is raised (the step's result is then invalid) and staging falls
+  // back to cp.async for the rest of the launch, so the kernel always finishes.
+  auto wait_plane = [&]() {
+    if (!pending_tma) {
+      cp_async_wait_all();
+      return;
+    }
+    unsigned done = 0;
+    for (int it = 0; it < (1 << 22) && !done; ++it) {
+      asm volatile(
+          "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+          : "=r"(done)
+          : "r"(bar_addr), "r"(tma_phase)
+          : "memory");
+    }
+    if (!done) {
+      *tma_off = 1;  // read by every loader after the next loader barrier
+      if (lt == 0 && a.status != nullptr) atomicOr(a.status, 1u);
+    }
+    tma_phase ^= 1u;
   };
   // Raw conserved -> primitive (reflecting walls flip the normal components first); loaders.
   auto convert_plane = [&](int zp, float* dst) {
@@ -159,7 +217,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
 #pragma unroll
     for (int k = 0; k < S::KL; ++k) {
       const int e = lt + k * S::NL;
-      if (e < PP) {
+      if (e < S::PW) {
         const int fl = sidx[(2 * k + 1) * S::NL + lt];
         const float fx = (fl & 1) ? -1.0f : 1.0f, fy = (fl & 2) ? -1.0f : 1.0f;
         F9 u;
@@ -189,7 +247,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   if (loader) {
     for (int zp = z0 - 2; zp <= z0; ++zp) {
       issue_plane(zp);
-      cp_async_wait_all();
+      wait_plane();
       loader_sync();
       convert_plane(zp, slot(zp));
       loader_sync();
@@ -214,7 +272,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   };
   // this thread's cell in the staged plane (halo lanes beyond 2*TY read a valid dummy cell)
   const int r0 = halo_warp ? (halo_act ? hrow + 2 : 2) : w + 1;
-  const int c0 = halo_warp ? (hside ? TILE_X + 2 : 1) : lane + 2;
+  const int c0 = halo_warp ? (hside ? PLANE_X0 + TILE_X : PLANE_X0 - 1) : PLANE_X0 + lane;
 
   // Conservative update of cell (x, y, pz) from its x/y divergence and its two z fluxes.
   auto update_cell = [&](int pz, const F9& dxy, const F9& flo, const F9& fhi) {
@@ -360,7 +418,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     }  // mid || row_own
     // ---- loaders: convert plane p+2 (its ring slot last held p-2) and prefetch p+3 -----------
     if (loader && p + 2 <= z1 + 1) {
-      cp_async_wait_all();
+      wait_plane();
       loader_sync();
       convert_plane(p + 2, slot(p + 2));
       loader_sync();
@@ -439,6 +497,17 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   cp_async_wait_all();
 }
 
+// The staging mbarrier (one arrival per TMA plane, the loads' bytes as its transaction).
+__device__ __forceinline__ void init_tma_barrier(unsigned long long* bar, int* off) {
+  if (threadIdx.x == 0) {
+    *off = 0;
+    const unsigned addr = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(addr) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+}
+
 // Block-wide max of v and one atomicMax into *bits (every thread of the CTA calls it).
 template <int NT>
 __device__ __forceinline__ void flush_smax(float v, unsigned int* bits) {
@@ -466,7 +535,11 @@ __device__ __forceinline__ void cta_range(long long Q, long long* q0, long long*
 // One box: a persistent launch of one CTA per resident slot.
 template <int TY, int RECON, int RSOL, bool CT, bool COMP>
 __global__ void __launch_bounds__(step_threads<TY>(), 1) mhd_step_kernel(const __grid_constant__ StepArgs a) {
-  extern __shared__ float smem[];
+  extern __shared__ __align__(128) float smem[];
+  __shared__ unsigned long long tma_bar;
+  __shared__ int tma_off;
+  unsigned tma_phase = 0;
+  init_tma_barrier(&tma_bar, &tma_off);
   long long q, qe;
   cta_range((long long)a.ntx * a.nty * a.nz, &q, &qe);
   float smax = 0.0f;
@@ -474,7 +547,8 @@ __global__ void __launch_bounds__(step_threads<TY>(), 1) mhd_step_kernel(const _
     const int col = (int)(q / a.nz);
     const int z0 = (int)(q - (long long)col * a.nz);
     const int z1 = (int)min((long long)a.nz, z0 + (qe - q));
-    march_column<TY, RECON, RSOL, CT, COMP>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax);
+    march_column<TY, RECON, RSOL, CT, COMP>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar, tma_phase,
+                                            &tma_off);
     q += z1 - z0;
   }
   if (!CT && a.smax_bits != nullptr) flush_smax<step_threads<TY>()>(smax, a.smax_bits);
@@ -482,7 +556,7 @@ __global__ void __launch_bounds__(step_threads<TY>(), 1) mhd_step_kernel(const _
 
 // Many boxes in one launch: box b owns global indices [q0_b, q0_{b+1}) of the concatenated
 // (column, plane) spaces; each CTA walks its equal share across box boundaries.
-struct BoxStep {
+struct alignas(64) BoxStep {
   StepArgs a;     // per-box pointers, extents and parameters; dscal = that box's {dt/dx, ch, decay}
   long long q0;   // first global (column, plane) index of this box
 };
@@ -490,10 +564,14 @@ struct BoxStep {
 template <int TY, int RECON, int RSOL, bool CT, bool COMP>
 __global__ void __launch_bounds__(step_threads<TY>(), 1) mhd_batch_kernel(const BoxStep* __restrict__ boxes, int nbox,
                                                                        long long Q) {
-  extern __shared__ float smem[];
+  extern __shared__ __align__(128) float smem[];
+  __shared__ unsigned long long tma_bar;
+  __shared__ int tma_off;
+  unsigned tma_phase = 0;
   long long q, qe;
   cta_range(Q, &q, &qe);
   if (q >= qe) return;
+  init_tma_barrier(&tma_bar, &tma_off);
   int b = 0, hi = nbox - 1;
   while (b < hi) {  // last box with q0 <= q
     const int mid = (b + hi + 1) >> 1;
@@ -512,7 +590,8 @@ __global__ void __launch_bounds__(step_threads<TY>(), 1) mhd_batch_kernel(const 
     const int col = (int)(local / a.nz);
     const int z0 = (int)(local - (long long)col * a.nz);
     const int z1 = (int)min((long long)a.nz, z0 + (qe - q));
-    march_column<TY, RECON, RSOL, CT, COMP>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax);
+    march_column<TY, RECON, RSOL, CT, COMP>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar, tma_phase,
+                                            &tma_off);
     q += z1 - z0;
   }
   if (!CT && boxes[b].a.smax_bits != nullptr) flush_smax<step_threads<TY>()>(smax, boxes[b].a.smax_bits);

@@ -79,6 +79,7 @@ SIGNATURES = {
                             ctypes.POINTER(ctypes.c_float)], ctypes.c_int),
     "pmfmhd_batch_destroy": ([_VP], ctypes.c_int),
     "pmfmhd_autotune": ([_VP, _GP, _P9, ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
+    "pmfmhd_status": ([_VP, ctypes.c_int, _VP], ctypes.c_int),
     "pmfmhd_set_tile": ([_VP, _GP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "pmfmhd_get_tile": ([_VP, _GP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                          ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
@@ -360,6 +361,11 @@ def get_tile(s: MHDState):
                                  1 if s.resid is not None else 0, ctypes.byref(rows), ctypes.byref(planes)),
            "get_tile")
     return rows.value, planes.value
+
+
+def device_status(s: MHDState, clear: bool = True) -> int:
+    """0, or the PMFMHD_ETIMEOUT code if a step's bounded TMA wait gave up since the last check."""
+    return lib().pmfmhd_status(context(s.device), int(clear), _stream())
 
 
 def max_divb(s: MHDState) -> float:

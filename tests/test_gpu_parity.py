@@ -243,3 +243,19 @@ def test_ct_compensated_faces_match_oracle():
     assert not within_parity(cpu.U, pmfmhd.fields_to_host(dev))
     rb = torch.stack([dev.ct.rbx, dev.ct.rby, dev.ct.rbz]).cpu().numpy()
     assert np.abs(rb).max() > 0
+
+
+def test_tma_staged_interior_matches_oracle_and_status_is_clear():
+    """A box large enough for TMA-staged interior tiles (x extent a multiple of 4, more than
+    40 cells): the result still matches the oracle and no bounded TMA wait gave up."""
+    dims = (96, 40, 24)
+    U = problems.turb_field(dims, 1.0 / 96)
+    cpu = oracle_state(U, dims)
+    dev = gpu_state(U, dims)
+    pmfmhd.device_status(dev, clear=True)
+    dt, speed = cpu.compute_dt(0.2)
+    for _ in range(3):
+        cpu.step(dt, ch=speed)
+        pmfmhd.step(dev, float(dt), ch=float(speed))
+    assert not within_parity(cpu.U, pmfmhd.fields_to_host(dev))
+    assert pmfmhd.device_status(dev) == 0
