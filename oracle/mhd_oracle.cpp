@@ -278,6 +278,59 @@ template <class T> T comp_update(T* r, long idx, T x, T dx) {
   return upd;
 }
 
+// ---- linear (Compton) drag toward a target velocity (glm_physics.jl:63-172) ------------
+template <class T> T drag_phi1(T q) { return std::fabs(q) < T(1e-4) ? T(1) - q / T(2) + q * q / T(6) : -std::expm1(-q) / q; }
+template <class T> void drag_work_coefficients(T q, T& A, T& C, T& D) {
+  if (q < T(0.05)) {
+    T q2 = q * q, q3 = q2 * q, q4 = q3 * q;
+    A = q * (T(1) - q + T(2.0 / 3.0) * q2 - T(1.0 / 3.0) * q3 + T(2.0 / 15.0) * q4);
+    C = q * (T(1) - q + T(7.0 / 12.0) * q2 - T(1.0 / 4.0) * q3 + T(31.0 / 360.0) * q4);
+    D = q * (T(1.0 / 3.0) - q / T(4) + T(7.0 / 60.0) * q2 - q3 / T(24) + T(31.0 / 2520.0) * q4);
+    return;
+  }
+  T em1 = -std::expm1(-q), em2 = -std::expm1(-T(2) * q);
+  A = T(0.5) * em2;
+  C = em1 * em1 / q;
+  D = (q - T(2) * em1 + T(0.5) * em2) / (q * q);
+}
+template <class T> struct Drag {
+  bool on;
+  T qh, q;     // half-step and full-step impulse
+  T v0[3];     // target velocity
+};
+// exact constant-force propagation of a face prediction (glm_physics.jl:71-84)
+template <class T> Q<T> drag_predict_face(const Q<T>& q0, const Q<T>& qh, T impulse, const T* v0) {
+  T decay = std::exp(-impulse), phi1 = drag_phi1(impulse);
+  Q<T> r = qh;
+  for (int c = 0; c < 3; ++c) r[1 + c] = v0[c] + decay * (q0[1 + c] - v0[c]) + phi1 * (qh[1 + c] - q0[1 + c]);
+  return r;
+}
+// cell corrector: exact momentum response and integrated drag work (glm_physics.jl:128-172)
+template <class T> Q<T> drag_correct_conserved(const Q<T>& u0, const Q<T>& trial, T impulse, const T* v0, T smallr,
+                                               T smallE) {
+  T decay = std::exp(-impulse), phi1 = drag_phi1(impulse), A, C, D;
+  drag_work_coefficients(impulse, A, C, D);
+  T rn = mx(trial[0], smallr), ro = mx(u0[0], smallr);
+  T vo[3] = {u0[1] / ro, u0[2] / ro, u0[3] / ro};
+  T vt[3] = {trial[1] / rn, trial[2] / rn, trial[3] / rn};
+  T dv[3], w[3], vn[3], iw[3];
+  for (int c = 0; c < 3; ++c) {
+    dv[c] = vt[c] - vo[c];
+    w[c] = vo[c] - v0[c];
+    vn[c] = v0[c] + decay * w[c] + phi1 * dv[c];
+    iw[c] = (T(1) - decay) * w[c] + (T(1) - phi1) * dv[c];
+  }
+  T w2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+  T wdv = w[0] * dv[0] + w[1] * dv[1] + w[2] * dv[2];
+  T dv2 = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
+  T qwork = rn * (A * w2 + C * wdv + D * dv2 + v0[0] * iw[0] + v0[1] * iw[1] + v0[2] * iw[2]);
+  T nm[3] = {rn * vn[0], rn * vn[1], rn * vn[2]};
+  T ek = T(0.5) * (nm[0] * nm[0] + nm[1] * nm[1] + nm[2] * nm[2]) / rn;
+  T eb = T(0.5) * (trial[5] * trial[5] + trial[6] * trial[6] + trial[7] * trial[7]);
+  T emin = ek + eb + smallE;
+  return Q<T>{{rn, nm[0], nm[1], nm[2], mx(trial[4] - qwork, emin), trial[5], trial[6], trial[7], trial[8]}};
+}
+
 // CT workspace slots (ct.jl:71-93 consumer order; state.jl:44-52 names)
 enum { W_MFX = 0, W_MFY, W_MFZ, W_FXBY, W_FXBZ, W_FYBX, W_FYBZ, W_FZBX, W_FZBY, W_ECX, W_ECY, W_ECZ, W_EX, W_EY, W_EZ, W_N };
 
@@ -286,7 +339,7 @@ enum { W_MFX = 0, W_MFY, W_MFZ, W_FXBY, W_FXBZ, W_FYBX, W_FYBZ, W_FZBX, W_FZBY, 
 //   CT: faces (3nc, lower-face normal B) and work (W_N*nc) non-NULL.
 template <class T>
 void godunov(const Grid& g, const T* U, T* Un, T dtdx, T ch, T decay, const Phys<T>& P, T* resid,
-             const T* faces, T* work) {
+             const T* faces, T* work, const Drag<T>& drag) {
   const long nc = (long)g.nx * g.ny * g.nz;
   const bool CT = faces != nullptr;
 #pragma omp parallel for schedule(dynamic, 64)
@@ -298,8 +351,12 @@ void godunov(const Grid& g, const T* U, T* Un, T dtdx, T ch, T decay, const Phys
     for (int d = 0; d < 3; ++d) {
       Edges<T> em = mh_edges(g, U, nc, i - off[d][0], j - off[d][1], k - off[d][2], dtdx, P);
       Edges<T> ep = mh_edges(g, U, nc, i + off[d][0], j + off[d][1], k + off[d][2], dtdx, P);
-      Q<T> Ll = qadd(em.mh, em.dR[d]), Rl = qadd(ec.mh, ec.dL[d]);
-      Q<T> Lh = qadd(ec.mh, ec.dR[d]), Rh = qadd(ep.mh, ep.dL[d]);
+      // face states mh + offset, drag-propagated when drag is on (integrator_ref.jl:28-39)
+      auto face = [&](const Edges<T>& e, const Q<T>& off) {
+        return drag.on ? drag_predict_face(qadd(e.m0, off), qadd(e.mh, off), drag.qh, drag.v0) : qadd(e.mh, off);
+      };
+      Q<T> Ll = face(em, em.dR[d]), Rl = face(ec, ec.dL[d]);
+      Q<T> Lh = face(ec, ec.dR[d]), Rh = face(ep, ep.dL[d]);
       if (CT) {
         T bl = faces[d * nc + c];
         T bh = faces[d * nc + per(g, i + off[d][0], j + off[d][1], k + off[d][2])];
@@ -315,7 +372,8 @@ void godunov(const Grid& g, const T* U, T* Un, T dtdx, T ch, T decay, const Phys
       work[W_FXBY * nc + c] = Fl[0][6]; work[W_FXBZ * nc + c] = Fl[0][7];
       work[W_FYBX * nc + c] = Fl[1][5]; work[W_FYBZ * nc + c] = Fl[1][7];
       work[W_FZBX * nc + c] = Fl[2][5]; work[W_FZBY * nc + c] = Fl[2][6];
-      const Q<T>& qc = ec.mh;
+      const Q<T> qz{{T(0), T(0), T(0), T(0), T(0), T(0), T(0), T(0), T(0)}};
+      const Q<T> qc = drag.on ? drag_predict_face(qadd(ec.m0, qz), qadd(ec.mh, qz), drag.qh, drag.v0) : ec.mh;
       work[W_ECX * nc + c] = qc[3] * U0[6] - qc[2] * U0[7];
       work[W_ECY * nc + c] = qc[1] * U0[7] - qc[3] * U0[5];
       work[W_ECZ * nc + c] = qc[2] * U0[5] - qc[1] * U0[6];
@@ -336,6 +394,7 @@ void godunov(const Grid& g, const T* U, T* Un, T dtdx, T ch, T decay, const Phys
       for (int v = 1; v < 8; ++v) r[v] = U0[v] + dU[v];
     }
     r[8] = U0[8] + dU[8];
+    if (drag.on) r = drag_correct_conserved(U0, r, drag.q, drag.v0, P.smallr, T(1e-30));  // integrator_ref.jl:155-156
     for (int v = 0; v < 8; ++v) Un[v * nc + c] = r[v];
     Un[8 * nc + c] = CT ? T(0) : r[8] * decay;
   }
@@ -497,14 +556,32 @@ struct oracle_params {
     return Phys<T>{T(p->gamma), T(p->smallr), T(p->pfl), T(p->llf_dmin), T(p->llf_pmin), p->recon, p->riemann}; \
   }                                                                                                        \
   static Grid grid_##SUF(const oracle_params* p) { return Grid{p->nx, p->ny, p->nz, {p->bc[0], p->bc[1], p->bc[2]}}; } \
+  static Drag<T> no_drag_##SUF() { return Drag<T>{false, T(0), T(0), {T(0), T(0), T(0)}}; }                 \
+  static Drag<T> drag_##SUF(double q, const double* v0) {                                                  \
+    Drag<T> d{true, T(0.5) * T(q), T(q), {T(0), T(0), T(0)}};                                            \
+    if (v0) for (int c = 0; c < 3; ++c) d.v0[c] = T(v0[c]);                                               \
+    return d;                                                                                              \
+  }                                                                                                        \
   void oracle_step_glm_##SUF(const oracle_params* p, const T* U, T* Un, double dtdx, double ch, double decay, T* resid) { \
-    godunov<T>(grid_##SUF(p), U, Un, T(dtdx), T(ch), T(decay), phys_##SUF(p), resid, nullptr, nullptr);   \
+    godunov<T>(grid_##SUF(p), U, Un, T(dtdx), T(ch), T(decay), phys_##SUF(p), resid, nullptr, nullptr,    \
+               no_drag_##SUF());                                                                  \
+  }                                                                                                        \
+  void oracle_step_glm_drag_##SUF(const oracle_params* p, const T* U, T* Un, double dtdx, double ch, double decay, \
+                                  double q, const double* v0) {                                           \
+    godunov<T>(grid_##SUF(p), U, Un, T(dtdx), T(ch), T(decay), phys_##SUF(p), nullptr, nullptr, nullptr,  \
+               drag_##SUF(q, v0));                                                                         \
   }                                                                                                        \
   void oracle_step_ct_##SUF(const oracle_params* p, const T* U, T* Un, T* faces, T* work, double dtdx,      \
                             T* resid, T* face_resid) {                                                    \
     Grid g = grid_##SUF(p);                                                                               \
-    godunov<T>(g, U, Un, T(dtdx), T(0), T(1), phys_##SUF(p), resid, faces, work);                         \
+    godunov<T>(g, U, Un, T(dtdx), T(0), T(1), phys_##SUF(p), resid, faces, work, no_drag_##SUF()); \
     ct_update<T>(g, Un, faces, work, face_resid, T(dtdx));                                                \
+  }                                                                                                        \
+  void oracle_step_ct_drag_##SUF(const oracle_params* p, const T* U, T* Un, T* faces, T* work, double dtdx, \
+                                 double q, const double* v0) {                                            \
+    Grid g = grid_##SUF(p);                                                                               \
+    godunov<T>(g, U, Un, T(dtdx), T(0), T(1), phys_##SUF(p), nullptr, faces, work, drag_##SUF(q, v0));    \
+    ct_update<T>(g, Un, faces, work, nullptr, T(dtdx));                                                   \
   }                                                                                                        \
   double oracle_max_wavespeed_##SUF(const oracle_params* p, const T* U) {                                 \
     return (double)max_wavespeed<T>(grid_##SUF(p), U, phys_##SUF(p));                                     \

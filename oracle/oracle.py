@@ -51,6 +51,8 @@ def lib():
         for suf in ("f32", "f64"):
             getattr(_LIB, f"oracle_step_glm_{suf}").argtypes = [P, vp, vp, d, d, d, vp]
             getattr(_LIB, f"oracle_step_ct_{suf}").argtypes = [P, vp, vp, vp, vp, d, vp, vp]
+            getattr(_LIB, f"oracle_step_glm_drag_{suf}").argtypes = [P, vp, vp, d, d, d, d, vp]
+            getattr(_LIB, f"oracle_step_ct_drag_{suf}").argtypes = [P, vp, vp, vp, vp, d, d, vp]
             for name in ("max_wavespeed",):
                 f = getattr(_LIB, f"oracle_{name}_{suf}")
                 f.argtypes = [P, vp]
@@ -80,6 +82,7 @@ class OracleState:
         self.dx = self.T(dx)
         self.gamma = self.T(gamma)
         self.mhd_solver = mhd_solver
+        self.smallr = self.T(smallr)
         if mhd_solver == "ct" and any(b != "periodic" for b in bcs):
             raise ValueError("mhd_solver='ct' requires all-periodic boundaries")
         self.p = OracleParams(self.dims[0], self.dims[1], self.dims[2], (ctypes.c_int * 3)(*[BC[b] for b in bcs]),
@@ -110,6 +113,72 @@ class OracleState:
             self._f("step_glm")(ctypes.byref(self.p), _ptr(self.U), _ptr(self.scratch), float(dtdx),
                                 float(T(ch)), float(decay), _ptr(self.resid))
         self.U, self.scratch = self.scratch, self.U
+
+    def step_drag_godunov(self, dt, drag_impulse, ch=None, glm_cr=GLM_CR, target_velocity=(0.0, 0.0, 0.0)):
+        """Source-coupled Godunov step with linear drag (drag.jl:162-178, step_drag_godunov!;
+        the kernel arithmetic of glm_physics.jl:63-172 and integrator_ref.jl:28-39,135,155-156
+        is restated in mhd_oracle.cpp)."""
+        if not (np.isfinite(drag_impulse) and drag_impulse >= 0):
+            raise ValueError("drag impulse must be finite and non-negative")
+        T = self.T
+        dtdx = T(T(dt) / self.dx)
+        v0 = (ctypes.c_double * 3)(*[float(T(v)) for v in target_velocity])
+        if self.mhd_solver == "ct":
+            self._f("step_ct_drag")(ctypes.byref(self.p), _ptr(self.U), _ptr(self.scratch), _ptr(self.faces),
+                                    _ptr(self.work), float(dtdx), float(T(drag_impulse)), v0)
+        else:
+            decay = T(np.exp(T(-T(glm_cr) * T(ch) * T(dt) / self.dx)))
+            self._f("step_glm_drag")(ctypes.byref(self.p), _ptr(self.U), _ptr(self.scratch), float(dtdx),
+                                     float(T(ch)), float(decay), float(T(drag_impulse)), v0)
+        self.U, self.scratch = self.scratch, self.U
+
+    def _drag_phi1(self, q):
+        """glm_physics.jl:63-65 in the state precision."""
+        T = self.T
+        q = T(q)
+        if abs(q) < T(1e-4):
+            return T(T(T(1) - q / T(2)) + q * q / T(6))
+        return T(-np.expm1(-q) / q)
+
+    def apply_linear_drag(self, decay, target_velocity=(0.0, 0.0, 0.0), energy_residual=None):
+        """apply_linear_drag! (drag.jl:78-117), elementwise in the state precision."""
+        T = self.T
+        with np.errstate(all="ignore"):
+            U = self.U
+            r = np.maximum(U[0], T(self.smallr))
+            d = T(decay)
+            ek0 = T(0.5) * (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / r
+            for c in range(3):
+                t = r * T(target_velocity[c])
+                U[1 + c] = t + (U[1 + c] - t) * d
+            ek1 = T(0.5) * (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / r
+            if energy_residual is None:
+                e = U[4] + (ek1 - ek0)
+            else:
+                inc = (ek1 - ek0) + energy_residual
+                e = U[4] + inc
+                energy_residual[:] = inc - (e - U[4])
+            U[4] = np.maximum(e, T(1e-30))
+
+    def apply_exponential_drag_increment(self, old_U, drag_impulse, target_velocity=(0.0, 0.0, 0.0)):
+        """apply_exponential_drag_increment! (drag.jl:121-208) on the trial self.U."""
+        T = self.T
+        q = T(drag_impulse)
+        decay, phi1 = T(np.exp(-q)), self._drag_phi1(q)
+        with np.errstate(all="ignore"):
+            U = self.U
+            rn = np.maximum(U[0], T(self.smallr))
+            ro = np.maximum(old_U[0], T(self.smallr))
+            ek0 = T(0.5) * (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / rn
+            eb = T(0.5) * (U[5] * U[5] + U[6] * U[6] + U[7] * U[7])
+            nonkinetic = np.maximum(U[4] - ek0, eb + T(1e-30))
+            for c in range(3):
+                v0 = T(target_velocity[c])
+                vo = old_U[1 + c] / ro
+                vt = U[1 + c] / rn
+                U[1 + c] = rn * (v0 + decay * (vo - v0) + phi1 * (vt - vo))
+            ek1 = T(0.5) * (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / rn
+            U[4] = np.maximum(nonkinetic + ek1, eb + T(1e-30))
 
     def max_wavespeed(self):
         return self.T(self._f("max_wavespeed")(ctypes.byref(self.p), _ptr(self.U)))

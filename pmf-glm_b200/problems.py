@@ -124,3 +124,69 @@ def smooth_fields(n, gamma=5 / 3, dtype=np.float32):
     q = [1 + 0.02 * np.sin(x) * np.cos(y), 0.02 * np.sin(z), 0.02 * np.sin(x), 0.02 * np.sin(y),
          1 + 0.01 * np.cos(z), 0.3 + 0.02 * np.sin(y), 0.02 * np.sin(z), 0.02 * np.sin(x), 0 * x]
     return _finish(q, gamma, dtype)
+
+
+def drag_alfven(N, amp=1e-3, gamma=5 / 3):
+    """Standing Alfven mode of the drag test on an (N, 4, 4) grid, built in FP32 as the
+    reference does (test/inherited/test_drag_godunov.jl:16-27): rho = 1, p0 = 1, B = (1, by, 0)
+    with by = amp*cos(2 pi x), gas at rest."""
+    T = np.float32
+    dims = (N, 4, 4)
+    i, _, _ = cell_coords(dims)
+    x = ((i - 0.5) / N).astype(T)
+    by = (T(amp) * np.cos(T(2 * np.pi) * x)).astype(T)
+    U = np.zeros((9, x.size), T)
+    U[0] = 1
+    U[5] = 1
+    U[6] = by
+    U[4] = T(1) / (T(gamma) - T(1)) + T(0.5) * (T(1) + by * by)
+    return U
+
+
+def drag_alfven_exact(t, gamma_drag, kva):
+    """Amplitude factor of a drag-damped standing Alfven mode (test_drag_godunov.jl:1-14)."""
+    half = 0.5 * gamma_drag
+    if gamma_drag == 0:
+        return np.cos(kva * t)
+    if half < kva:
+        mu = np.sqrt(kva * kva - half * half)
+        return np.exp(-half * t) * (np.cos(mu * t) + half / mu * np.sin(mu * t))
+    if half > kva:
+        mu = np.sqrt(half * half - kva * kva)
+        rs, rf = -half + mu, -half - mu
+        return (-rf * np.exp(rs * t) + rs * np.exp(rf * t)) / (rs - rf)
+    return np.exp(-half * t) * (1 + half * t)
+
+
+def uniform_drift(n, rho=1.5, v=(0.7, -0.2, 0.1), B=(0.3, -0.1, 0.2), etherm=2.25):
+    """Uniform moving magnetised gas in FP32 (test/inherited/test_terminal_ct.jl:343-356)."""
+    T = np.float32
+    rho, etherm = T(rho), T(etherm)
+    v = [T(c) for c in v]
+    B = [T(c) for c in B]
+    U = np.zeros((9, n ** 3), T)
+    U[0] = rho
+    for d in range(3):
+        U[1 + d] = rho * v[d]
+        U[5 + d] = B[d]
+    U[4] = etherm + T(0.5) * rho * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) + T(0.5) * (
+        B[0] * B[0] + B[1] * B[1] + B[2] * B[2])
+    return U
+
+
+def ct_smoke_fields(N, gamma=5 / 3):
+    """Weakly perturbed CT smoke state (test/inherited/test_ct.jl:421-433), FP32."""
+    T = np.float32
+    g = T(gamma)
+    i, j, _ = cell_coords((N, N, N))
+    ph = (T(2) * T(np.pi) * (i - 1) / N).astype(T)
+    ph2 = (T(2) * T(np.pi) * (j - 1) / N).astype(T)
+    rho = T(1) + T(1e-2) * np.cos(ph)
+    vx = T(1e-2) * np.sin(ph)
+    bx = np.full_like(rho, T(0.5))
+    by = T(0.05) * np.sin(ph)
+    bz = T(0.03) * np.cos(ph2 + T(1))
+    U = np.zeros((9, rho.size), T)
+    U[0], U[1], U[5], U[6], U[7] = rho, rho * vx, bx, by, bz
+    U[4] = T(1) / (g - T(1)) + T(0.5) * rho * vx * vx + T(0.5) * (bx * bx + by * by + bz * bz)
+    return U

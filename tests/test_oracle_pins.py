@@ -127,3 +127,75 @@ def test_oracle_f32_tracks_f64():
     for v in range(8):
         err = np.abs(a.U[v] - b.U[v]).max() / np.abs(b.U[v]).max()
         assert err < 2e-5, (v, err)
+
+
+# ---- source-coupled drag (drag.jl, glm_physics.jl:63-172) ----------------------------------
+
+@pytest.mark.parametrize("gamma_drag", [0.0, 100.0, 1000.0])
+def test_drag_alfven_known_answer(gamma_drag):
+    """test/inherited/test_drag_godunov.jl:16-57: a standing Alfven mode under linear drag
+    follows the analytic damped oscillator (N=128x4x4, PPM/HLLD, dt=0.002 to t=0.1)."""
+    N = 128
+    s = oracle.OracleState((N, 4, 4), 1.0 / N, recon="ppm", riemann="hlld")
+    s.U[:] = problems.drag_alfven(N)
+    t = 0.0
+    while t < 0.1 - 1e-14:
+        dtn = min(0.002, 0.1 - t)
+        s.step_drag_godunov(dtn, gamma_drag * dtn, ch=1.5, glm_cr=0.0)
+        t += dtn
+    i = np.arange(N)
+    measured = 2.0 / N * np.sum(s.U[6][:N].astype(np.float64) * np.cos(2 * np.pi * (i + 0.5) / N))
+    exact = 1e-3 * problems.drag_alfven_exact(t, gamma_drag, 2 * np.pi)
+    assert np.isfinite(s.U[4]).all()
+    assert abs(measured - exact) / 1e-3 < (0.015 if gamma_drag == 0 else 0.025)
+
+
+@pytest.mark.parametrize("q", [1e-6, 1e-3, 0.1, 1.0, 10.0, 100.0])
+def test_drag_uniform_state_work_known_answer(q):
+    """test/inherited/test_terminal_ct.jl:343-370: on a uniform drifting state the step is
+    pure drag: v -> v e^-q, the thermal energy is kept, the work is rho v^2 (1-e^-2q)/2 and
+    the density is untouched."""
+    n, rho, v, B, eth = 8, 1.5, (0.7, -0.2, 0.1), (0.3, -0.1, 0.2), 2.25
+    s = oracle.OracleState((n, n, n), 1.0 / n, recon="ppm")
+    s.U[:] = problems.uniform_drift(n, rho, v, B, eth)
+    E0 = float(s.U[4][0])
+    s.step_drag_godunov(0.01, q, ch=1.0, glm_cr=0.0)
+    h = s.U.astype(np.float64)
+    T = np.float32
+    for d in range(3):
+        assert abs(h[1 + d][0] / h[0][0] - v[d] * np.exp(-q)) <= 2e-7 + 5e-6 * abs(v[d] * np.exp(-q))
+    ek = 0.5 * sum(h[1 + d][0] ** 2 for d in range(3)) / h[0][0]
+    eb = 0.5 * sum(T(b) ** 2 for b in B)
+    assert abs(h[4][0] - ek - eb - eth) <= 4e-6
+    work = 0.5 * rho * sum(c * c for c in v) * (1 - np.exp(-2 * q))
+    assert abs((E0 - h[4][0]) - work) <= 3e-7 + 8e-6 * work
+    assert np.all(s.U[0] == T(rho))
+
+
+def test_drag_zero_impulse_limit():
+    """test/inherited/test_terminal_ct.jl:372-381: zero impulse reproduces the plain step."""
+    n = 8
+    U = problems.alfven_wave((n, n, n), 1.0 / n, amp=0.05, B0=1.0, p0=0.2)
+    a = oracle.OracleState((n, n, n), 1.0 / n, recon="ppm")
+    b = oracle.OracleState((n, n, n), 1.0 / n, recon="ppm")
+    a.U[:] = U
+    b.U[:] = U
+    a.step(0.002, ch=1.5, glm_cr=0.3)
+    b.step_drag_godunov(0.002, 0.0, ch=1.5, glm_cr=0.3)
+    assert np.abs(a.U - b.U).max() < 2e-6
+
+
+def test_drag_operators_limits():
+    """apply_linear_drag with decay 1 and the exponential increment with impulse 0 leave a
+    state unchanged up to the floors; decay 0 stops the gas in the target frame."""
+    n = 6
+    U = problems.turb_field((n, n, n), 1.0 / n)
+    s = oracle.OracleState((n, n, n), 1.0 / n)
+    s.U[:] = U
+    s.apply_linear_drag(1.0)
+    assert np.array_equal(s.U, U)
+    s.apply_linear_drag(0.0, target_velocity=(0.1, 0.0, -0.2))
+    assert np.allclose(s.U[1] / s.U[0], 0.1, atol=1e-7) and np.allclose(s.U[3] / s.U[0], -0.2, atol=1e-7)
+    s.U[:] = U
+    s.apply_exponential_drag_increment(U.copy(), 0.0)
+    assert np.abs(s.U - U).max() <= 1e-6 * np.abs(U).max()
