@@ -96,6 +96,44 @@ int pmfmhd_step_ct(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9
                    float* ct_packed, float dt, float* const resid[7], int compensate_faces, void* stream);
 
 /*
+ * Source-coupled drag step: the GLM Godunov step above with linear (Compton) drag of
+ * impulse q = drag_impulse = Gamma*dt toward target_velocity (null = at rest) folded in.
+ * Replaces `step_ref_drag!` (integrator_ref.jl:222-234) and `step_cube_drag!`
+ * (integrator_cube.jl:478-490), the kernels behind `step_drag_godunov!` (drag.jl:162-178):
+ * the Hancock face states (and the CT cell EMF) carry the drag-propagated velocity
+ * v0 + exp(-q/2)(v - v0) + phi1(q/2)(v_half - v) (glm_physics.jl:71-84), and each cell's
+ * trial update is corrected by the exact momentum response and the integrated drag work
+ * (`drag_correct_conserved`, glm_physics.jl:128-172). No compensation (the reference passes
+ * no tracking flags), so a compensated state's remainders are left untouched.
+ * q must be finite and >= 0 (PMFMHD_EINVAL otherwise); q = 0 gives the plain step up to
+ * the density floor max(rho, smallr) of the corrector.
+ */
+int pmfmhd_step_glm_drag(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],
+                         float dt, float ch, float decay, float drag_impulse, const float target_velocity[3],
+                         void* stream);
+/* The CT form (step_ref_drag! on a mhd_solver=:ct state, then ct_update! without face
+ * compensation, integrator_ref.jl:222-234). */
+int pmfmhd_step_ct_drag(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],
+                        float* ct_packed, float dt, float drag_impulse, const float target_velocity[3],
+                        void* stream);
+/*
+ * In-place exact linear drag with velocity decay factor `decay` in [0, 1]
+ * (`apply_linear_drag!`, drag.jl:78-117): m <- rho v0 + (m - rho v0) decay with
+ * rho floored at smallr, E changed by the kinetic-energy change and floored at 1e-30.
+ * energy_residual (n cells, nullable) Kahan-compensates E as `energy_compensation`.
+ * Reads U[0..4] only.
+ */
+int pmfmhd_apply_linear_drag(pmfmhd_ctx* ctx, const pmfmhd_grid* g, float* const U[9], float decay,
+                             const float target_velocity[3], float* energy_residual, void* stream);
+/*
+ * In-place exponential constant-force correction of a no-drag trial U given the state
+ * before it (`apply_exponential_drag_increment!`, drag.jl:121-208). Reads old_U[0..3].
+ */
+int pmfmhd_apply_exponential_drag_increment(pmfmhd_ctx* ctx, const pmfmhd_grid* g, float* const U[9],
+                                            const float* const old_U[9], float drag_impulse,
+                                            const float target_velocity[3], void* stream);
+
+/*
  * Max signal speed max over cells and axes of |v_d| + c_fast,d (timestep.jl:4-14,
  * `max_wavespeed!` :17-23). Blocking; *smax receives the host value.
  */

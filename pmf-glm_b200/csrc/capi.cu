@@ -158,8 +158,8 @@ int occupancy_of(const StepKernelInfo& k) {
 }
 
 int launch_step(pmfmhd_ctx* c, const pmfmhd_grid* g, StepArgs& a, Tune t, bool ct, bool comp,
-                cudaStream_t s) {
-  StepKernelInfo k = step_kernel_info(t.ty, g->recon, g->riemann, ct, comp);
+                cudaStream_t s, bool drag = false) {
+  StepKernelInfo k = step_kernel_info(t.ty, g->recon, g->riemann, ct, comp, drag);
   if (k.fn == nullptr) return PMFMHD_EUNSUPPORTED;
   const int occ = occupancy_of(k);
   a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
@@ -189,24 +189,52 @@ void fill_glm_args(StepArgs& a, const float* const U[9], float* const Un[9], flo
   a.dscal = nullptr;
 }
 
+// Drag coefficients of one step with impulse q, in FP32 with the reference's formulas
+// (glm_physics.jl:63-66 _drag_phi1, :89-104 _drag_work_coefficients, :115-119 _drag_coefficients).
+float drag_phi1(float q) { return std::fabs(q) < 1e-4f ? 1.0f - q / 2.0f + q * q / 6.0f : -std::expm1(-q) / q; }
+
+DragCoef drag_coefficients(float q, const float* v0) {
+  DragCoef k;
+  for (int c = 0; c < 3; ++c) k.v0[c] = v0 ? v0[c] : 0.0f;
+  const float qh = 0.5f * q;
+  k.fdecay = std::exp(-qh);
+  k.fphi1 = drag_phi1(qh);
+  k.decay = std::exp(-q);
+  k.phi1 = drag_phi1(q);
+  if (q < 0.05f) {
+    const float q2 = q * q, q3 = q2 * q, q4 = q3 * q;
+    k.A = q * (1.0f - q + (2.0f / 3.0f) * q2 - (1.0f / 3.0f) * q3 + (2.0f / 15.0f) * q4);
+    k.C = q * (1.0f - q + (7.0f / 12.0f) * q2 - (1.0f / 4.0f) * q3 + (31.0f / 360.0f) * q4);
+    k.D = q * (1.0f / 3.0f - q / 4.0f + (7.0f / 60.0f) * q2 - q3 / 24.0f + (31.0f / 2520.0f) * q4);
+  } else {
+    const float em1 = -std::expm1(-q), em2 = -std::expm1(-2.0f * q);
+    k.A = 0.5f * em2;
+    k.C = em1 * em1 / q;
+    k.D = (q - 2.0f * em1 + 0.5f * em2) / (q * q);
+  }
+  return k;
+}
+
 int enqueue_glm(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Un[9], float dt,
-                float ch, float decay, float* const resid[7], bool comp, cudaStream_t s) {
+                float ch, float decay, float* const resid[7], bool comp, cudaStream_t s, const DragCoef* drag) {
   StepArgs a;
   const float dtdx = dt / g->dx;  // T(dt)/s.dx (integrator_ref.jl:211)
   fill_glm_args(a, U, Un, resid, comp, dtdx, ch, decay, c->d_smax);
+  if (drag) a.drag = *drag;
   PMF_CK(cudaMemsetAsync(c->d_smax, 0, sizeof(unsigned int), s));
-  return launch_step(c, g, a, tune_for(c, g, false, comp), false, comp, s);
+  return launch_step(c, g, a, tune_for(c, g, false, comp), false, comp, s, drag != nullptr);
 }
 
 int enqueue_ct(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Un[9], float* ct, float dt,
-               float* const resid[7], bool comp, bool comp_faces, cudaStream_t s) {
+               float* const resid[7], bool comp, bool comp_faces, cudaStream_t s, const DragCoef* drag) {
   const long long nc = ncells(g);
   const float dtdx = dt / g->dx;
   StepArgs a;
   fill_glm_args(a, U, Un, resid, comp, dtdx, 0.0f, 1.0f, nullptr);
+  if (drag) a.drag = *drag;
   for (int d = 0; d < 3; ++d) a.face[d] = ct + (size_t)(CT_BXF + d) * nc;
   for (int k = 0; k < CT_NWORK; ++k) a.work[k] = ct + (size_t)(CT_MFX + k) * nc;
-  int rc = launch_step(c, g, a, tune_for(c, g, true, comp), true, comp, s);
+  int rc = launch_step(c, g, a, tune_for(c, g, true, comp), true, comp, s, drag != nullptr);
   if (rc != PMFMHD_OK) return rc;
   const int nb = aux_blocks(c, nc);
   ct_emf_kernel<<<nb, AUX_THREADS, 0, s>>>(ct, g->nx, g->ny, g->nz);
@@ -300,7 +328,7 @@ int pmfmhd_step_glm(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9]
   if (!std::isfinite(dt) || !std::isfinite(ch) || !std::isfinite(decay) || !(ch > 0.0f)) return PMFMHD_EINVAL;
   bool comp;
   if ((rc = resid_mode(resid, &comp))) return rc;
-  return enqueue_glm(c, g, U, Unew, dt, ch, decay, resid, comp, as_stream(stream));
+  return enqueue_glm(c, g, U, Unew, dt, ch, decay, resid, comp, as_stream(stream), nullptr);
 }
 
 int pmfmhd_step_ct(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],
@@ -313,7 +341,34 @@ int pmfmhd_step_ct(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9],
   if (!std::isfinite(dt)) return PMFMHD_EINVAL;
   bool comp;
   if ((rc = resid_mode(resid, &comp))) return rc;
-  return enqueue_ct(c, g, U, Unew, ct_packed, dt, resid, comp, compensate_faces != 0, as_stream(stream));
+  return enqueue_ct(c, g, U, Unew, ct_packed, dt, resid, comp, compensate_faces != 0, as_stream(stream), nullptr);
+}
+
+int pmfmhd_step_glm_drag(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],
+                         float dt, float ch, float decay, float drag_impulse, const float target_velocity[3],
+                         void* stream) {
+  if (c == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!nonnull(U, 9) || !nonnull(Unew, 9)) return PMFMHD_EINVAL;
+  if (!std::isfinite(dt) || !std::isfinite(ch) || !std::isfinite(decay) || !(ch > 0.0f)) return PMFMHD_EINVAL;
+  if (!std::isfinite(drag_impulse) || !(drag_impulse >= 0.0f)) return PMFMHD_EINVAL;
+  const DragCoef k = drag_coefficients(drag_impulse, target_velocity);
+  return enqueue_glm(c, g, U, Unew, dt, ch, decay, nullptr, false, as_stream(stream), &k);
+}
+
+int pmfmhd_step_ct_drag(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],
+                        float* ct_packed, float dt, float drag_impulse, const float target_velocity[3],
+                        void* stream) {
+  if (c == nullptr || ct_packed == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!all_periodic(g)) return PMFMHD_EUNSUPPORTED;
+  if (!nonnull(U, 9) || !nonnull(Unew, 9)) return PMFMHD_EINVAL;
+  if (!std::isfinite(dt)) return PMFMHD_EINVAL;
+  if (!std::isfinite(drag_impulse) || !(drag_impulse >= 0.0f)) return PMFMHD_EINVAL;
+  const DragCoef k = drag_coefficients(drag_impulse, target_velocity);
+  return enqueue_ct(c, g, U, Unew, ct_packed, dt, nullptr, false, false, as_stream(stream), &k);
 }
 
 int pmfmhd_max_wavespeed(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* smax, void* stream) {

@@ -84,5 +84,7 @@ Tune tune_for(pmfmhd_ctx* c, const pmfmhd_grid* g, bool ct, bool comp);
 // for this grid (x extent not a multiple of 4, unaligned pointers, box larger than the grid).
 bool field_maps(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], int ty, CUtensorMap out[9]);
 int aux_blocks(const pmfmhd_ctx* c, long long nc);
+// Drag coefficients of one step with impulse q toward `v0` (null: at rest), FP32.
+DragCoef drag_coefficients(float q, const float* v0);
 }  // namespace host
 }  // namespace pmf

@@ -416,6 +416,68 @@ __device__ __forceinline__ float cell_wavespeed(const F9& u, const Phys& P) {
 
 // Kahan-compensated accumulation with a persistent remainder (glm_physics.jl:349-359).
 // The fast-math build must not reassociate it, so the rounding steps are explicit.
+// ---- linear (Compton) drag toward a target velocity, glm_physics.jl:63-172 ------------------
+// Coefficients of one step with impulse q = Gamma*dt (computed on the host in FP32 with the
+// reference's formulas): the face prediction uses the half-step pair (exp(-q/2), phi1(q/2)),
+// the cell corrector the full-step pair and the integrated-work coefficients A, C, D.
+struct DragCoef {
+  float v0[3];       // target velocity
+  float fdecay, fphi1;
+  float decay, phi1, A, C, D;
+};
+
+// Drag-propagated Hancock prediction (glm_physics.jl:71-84 with the face offset folded):
+// the face velocity v0 + fd*((m0+d) - v0) + fp*((mh+d) - (m0+d)) equals mh' + fd*d with
+// mh' = v0 + fd*(m0 - v0) + fp*(mh - m0), so the cell's predicted velocity is replaced by mh'
+// and its velocity offsets are scaled by fd. Density, pressure, B and psi keep their
+// hyperbolic midpoint values.
+template <int RECON>
+__device__ __forceinline__ void drag_predict_cell(F9& mh, const F9& m0, Offsets<RECON>& ox, Offsets<RECON>& oy,
+                                                  Offsets<RECON>& oz, const DragCoef& k) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float v0 = k.v0[c];
+    mh[1 + c] = v0 + k.fdecay * (m0[1 + c] - v0) + k.fphi1 * (mh[1 + c] - m0[1 + c]);
+    ox.dR[1 + c] *= k.fdecay;
+    oy.dR[1 + c] *= k.fdecay;
+    oz.dR[1 + c] *= k.fdecay;
+    if constexpr (RECON == RECON_PPM) {
+      ox.dL[1 + c] *= k.fdecay;
+      oy.dL[1 + c] *= k.fdecay;
+      oz.dL[1 + c] *= k.fdecay;
+    }
+  }
+}
+
+// Cell corrector (glm_physics.jl:128-172): exact momentum response to the trial velocity
+// increment and the analytically integrated drag work removed from E, with the density
+// floored at smallr and E floored at the new kinetic + magnetic energy + 1e-30.
+__device__ __forceinline__ void drag_correct_cell(const F9& u0, F9& t, const DragCoef& k, float smallr) {
+  const float rn = fmaxf(t[0], smallr), ro = fmaxf(u0[0], smallr);
+  float w[3], dv[3], vn[3], iw[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float vo = u0[1 + c] / ro, vt = t[1 + c] / rn;
+    dv[c] = vt - vo;
+    w[c] = vo - k.v0[c];
+    vn[c] = k.v0[c] + k.decay * w[c] + k.phi1 * dv[c];
+    iw[c] = (1.0f - k.decay) * w[c] + (1.0f - k.phi1) * dv[c];
+  }
+  const float w2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+  const float wdv = w[0] * dv[0] + w[1] * dv[1] + w[2] * dv[2];
+  const float dv2 = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
+  const float qwork =
+      rn * (k.A * w2 + k.C * wdv + k.D * dv2 + k.v0[0] * iw[0] + k.v0[1] * iw[1] + k.v0[2] * iw[2]);
+  const float nm0 = rn * vn[0], nm1 = rn * vn[1], nm2 = rn * vn[2];
+  const float ek = 0.5f * (nm0 * nm0 + nm1 * nm1 + nm2 * nm2) / rn;
+  const float eb = 0.5f * (t[5] * t[5] + t[6] * t[6] + t[7] * t[7]);
+  t[0] = rn;
+  t[1] = nm0;
+  t[2] = nm1;
+  t[3] = nm2;
+  t[4] = fmaxf(t[4] - qwork, ek + eb + 1e-30f);
+}
+
 __device__ __forceinline__ float comp_add(float x, float dx, float& r) {
   float inc = __fadd_rn(dx, r);
   float upd = __fadd_rn(x, inc);

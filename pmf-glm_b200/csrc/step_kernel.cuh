@@ -55,6 +55,7 @@ struct StepArgs {
   unsigned int* status;     // device status bits (1: a bounded wait for a TMA load gave up), or null
   int use_tma;              // the tensor maps below describe U (fields with nx % 4 == 0)
   CUtensorMap tmap[9];      // per field: 3-D (x, y, z) FP32 map, box (PLANE_W, TY+4, 1)
+  DragCoef drag;            // source-coupled drag step: coefficients (read only by DRAG kernels)
 };
 
 template <int TY>
@@ -84,10 +85,11 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // One column segment: planes [z0, z1) of column tile (tx, ty) of the box described by `a`.
 // Every thread of the CTA calls it; `smax` accumulates the new state's max signal speed.
-template <int TY, int RECON, int RSOL, bool CT, bool COMP>
+template <int TY, int RECON, int RSOL, bool CT, bool COMP, bool DRAG>
 __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, int z0, int z1, float* smem,
                                              float& smax, unsigned long long* tma_bar, unsigned& tma_phase,
                                              int* tma_off) {
+  static_assert(!(DRAG && COMP), "the drag step updates without compensation");
   using S = StepSmem<TY>;
   constexpr int NT = step_threads<TY>();
   constexpr int PP = S::PP;
@@ -304,6 +306,9 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
 #pragma unroll
       for (int i = 1; i <= 7; ++i) un[i] = u0[i] + d[i];
     }
+    // drag corrector on the uncompensated trial (its energy floor reads the trial cell B,
+    // which CT later replaces by the face average); integrator_ref.jl:155-156
+    if constexpr (DRAG) drag_correct_cell(u0, un, a.drag, P.smallr);
     un[8] = CT ? 0.0f : (u0[8] + d[8]) * decay;
 #pragma unroll
     for (int f = 0; f < 9; ++f) {
@@ -360,6 +365,9 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       for (int i = 0; i < 9; ++i) uh[i] = u0[i] - h * acc[i];
       mh = cons2prim(uh, g, P.smallr, P.pfl);
     }
+    // drag: face states and the CT cell EMF see the drag-propagated velocity
+    // (integrator_ref.jl:28-31,135)
+    if constexpr (DRAG) drag_predict_cell<RECON>(mh, m0, ox, oy, oz, a.drag);
     if constexpr (CT) {
       // cell-centred reference EMF -v x B: v of the predicted state, B at the start of the
       // step (integrator_ref.jl:133-138)
@@ -533,7 +541,7 @@ __device__ __forceinline__ void cta_range(long long Q, long long* q0, long long*
 }
 
 // One box: a persistent launch of one CTA per resident slot.
-template <int TY, int RECON, int RSOL, bool CT, bool COMP>
+template <int TY, int RECON, int RSOL, bool CT, bool COMP, bool DRAG>
 __global__ void __launch_bounds__(step_threads<TY>(), 1) mhd_step_kernel(const __grid_constant__ StepArgs a) {
   extern __shared__ __align__(128) float smem[];
   __shared__ unsigned long long tma_bar;
@@ -547,8 +555,8 @@ __global__ void __launch_bounds__(step_threads<TY>(), 1) mhd_step_kernel(const _
     const int col = (int)(q / a.nz);
     const int z0 = (int)(q - (long long)col * a.nz);
     const int z1 = (int)min((long long)a.nz, z0 + (qe - q));
-    march_column<TY, RECON, RSOL, CT, COMP>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar, tma_phase,
-                                            &tma_off);
+    march_column<TY, RECON, RSOL, CT, COMP, DRAG>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar,
+                                                  tma_phase, &tma_off);
     q += z1 - z0;
   }
   if (!CT && a.smax_bits != nullptr) flush_smax<step_threads<TY>()>(smax, a.smax_bits);
@@ -590,8 +598,8 @@ __global__ void __launch_bounds__(step_threads<TY>(), 1) mhd_batch_kernel(const 
     const int col = (int)(local / a.nz);
     const int z0 = (int)(local - (long long)col * a.nz);
     const int z1 = (int)min((long long)a.nz, z0 + (qe - q));
-    march_column<TY, RECON, RSOL, CT, COMP>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar, tma_phase,
-                                            &tma_off);
+    march_column<TY, RECON, RSOL, CT, COMP, false>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar,
+                                                   tma_phase, &tma_off);
     q += z1 - z0;
   }
   if (!CT && boxes[b].a.smax_bits != nullptr) flush_smax<step_threads<TY>()>(smax, boxes[b].a.smax_bits);

@@ -6,9 +6,11 @@
 namespace pmf {
 namespace detail {
 template <int TY, int RECON, int RSOL>
-StepKernel pick(bool ct, bool comp) {
-  if (ct) return comp ? mhd_step_kernel<TY, RECON, RSOL, true, true> : mhd_step_kernel<TY, RECON, RSOL, true, false>;
-  return comp ? mhd_step_kernel<TY, RECON, RSOL, false, true> : mhd_step_kernel<TY, RECON, RSOL, false, false>;
+StepKernel pick(bool ct, bool comp, bool drag) {
+  if (drag) return ct ? mhd_step_kernel<TY, RECON, RSOL, true, false, true> : mhd_step_kernel<TY, RECON, RSOL, false, false, true>;
+  if (ct)
+    return comp ? mhd_step_kernel<TY, RECON, RSOL, true, true, false> : mhd_step_kernel<TY, RECON, RSOL, true, false, false>;
+  return comp ? mhd_step_kernel<TY, RECON, RSOL, false, true, false> : mhd_step_kernel<TY, RECON, RSOL, false, false, false>;
 }
 template <int TY, int RECON, int RSOL>
 BatchKernel pick_batch(bool ct, bool comp) {
@@ -34,21 +36,21 @@ BatchKernel batch(int recon, int rsol, bool ct, bool comp) {
   return nullptr;
 }
 template <int TY, int RECON>
-StepKernel pick_rs(int rsol, bool ct, bool comp) {
+StepKernel pick_rs(int rsol, bool ct, bool comp, bool drag) {
   switch (rsol) {
-    case RS_HLLD: return pick<TY, RECON, RS_HLLD>(ct, comp);
-    case RS_HLL: return pick<TY, RECON, RS_HLL>(ct, comp);
-    case RS_LLF: return pick<TY, RECON, RS_LLF>(ct, comp);
+    case RS_HLLD: return pick<TY, RECON, RS_HLLD>(ct, comp, drag);
+    case RS_HLL: return pick<TY, RECON, RS_HLL>(ct, comp, drag);
+    case RS_LLF: return pick<TY, RECON, RS_LLF>(ct, comp, drag);
   }
   return nullptr;
 }
 template <int TY>
-StepKernelInfo info(int recon, int rsol, bool ct, bool comp) {
+StepKernelInfo info(int recon, int rsol, bool ct, bool comp, bool drag) {
   StepKernelInfo k{nullptr, StepSmem<TY>::BYTES, step_threads<TY>()};
   switch (recon) {
-    case RECON_PLM: k.fn = pick_rs<TY, RECON_PLM>(rsol, ct, comp); break;
-    case RECON_PPM: k.fn = pick_rs<TY, RECON_PPM>(rsol, ct, comp); break;
-    case RECON_PLM_MINMOD: k.fn = pick_rs<TY, RECON_PLM_MINMOD>(rsol, ct, comp); break;
+    case RECON_PLM: k.fn = pick_rs<TY, RECON_PLM>(rsol, ct, comp, drag); break;
+    case RECON_PPM: k.fn = pick_rs<TY, RECON_PPM>(rsol, ct, comp, drag); break;
+    case RECON_PLM_MINMOD: k.fn = pick_rs<TY, RECON_PLM_MINMOD>(rsol, ct, comp, drag); break;
   }
   return k;
 }

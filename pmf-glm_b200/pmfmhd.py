@@ -5,7 +5,10 @@ The names, arguments and error behaviour follow lib/MHDKernels/src: ``allocate_s
 integrator_cube.jl:455-463, integrator_ref.jl:210-220), ``evolve`` (driver.jl:48-71),
 ``compute_dt`` / ``max_wavespeed`` (timestep.jl:17-46), ``max_divb`` /
 ``conserved_totals`` (diagnostics.jl:22-55), ``max_divb_face`` / ``ct_faces_from_potential``
-/ ``ct_faces_from_cells`` (ct.jl:187-345). Errors raise ``PMFMHDError`` where the
+/ ``ct_faces_from_cells`` (ct.jl:187-345), the drag steps and operators of drag.jl
+(``step_drag_godunov``, ``step_ref_drag`` / ``step_cube_drag``, ``apply_linear_drag``,
+``apply_exponential_drag_increment``, ``step_drag_strang``, ``step_drag_exponential``,
+``DragRegimeController`` / ``update_drag_regime``). Errors raise ``PMFMHDError`` where the
 reference calls ``error(...)``. Every step runs the sm_100a CUDA library; there is no CPU
 path, and a missing library raises at import of the first call.
 """
@@ -54,6 +57,8 @@ _P9 = ctypes.c_void_p * 9
 _P7 = ctypes.c_void_p * 7
 _P3 = ctypes.c_void_p * 3
 _GP = ctypes.POINTER(Grid)
+_F3P = ctypes.POINTER(ctypes.c_float)  # const float[3], nullable
+
 SIGNATURES = {
     "pmfmhd_version": ([], ctypes.c_int),
     "pmfmhd_strerror": ([ctypes.c_int], ctypes.c_char_p),
@@ -62,6 +67,11 @@ SIGNATURES = {
     "pmfmhd_destroy": ([_VP], ctypes.c_int),
     "pmfmhd_step_glm": ([_VP, _GP, _P9, _P9, ctypes.c_float, ctypes.c_float, ctypes.c_float, _VP, _VP], ctypes.c_int),
     "pmfmhd_step_ct": ([_VP, _GP, _P9, _P9, _VP, ctypes.c_float, _VP, ctypes.c_int, _VP], ctypes.c_int),
+    "pmfmhd_step_glm_drag": ([_VP, _GP, _P9, _P9, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                              _F3P, _VP], ctypes.c_int),
+    "pmfmhd_step_ct_drag": ([_VP, _GP, _P9, _P9, _VP, ctypes.c_float, ctypes.c_float, _F3P, _VP], ctypes.c_int),
+    "pmfmhd_apply_linear_drag": ([_VP, _GP, _P9, ctypes.c_float, _F3P, _VP, _VP], ctypes.c_int),
+    "pmfmhd_apply_exponential_drag_increment": ([_VP, _GP, _P9, _P9, ctypes.c_float, _F3P, _VP], ctypes.c_int),
     "pmfmhd_max_wavespeed": ([_VP, _GP, _P9, ctypes.POINTER(ctypes.c_float), _VP], ctypes.c_int),
     "pmfmhd_compute_dt": ([_VP, _GP, _P9, ctypes.c_float, ctypes.POINTER(ctypes.c_float),
                            ctypes.POINTER(ctypes.c_float), _VP], ctypes.c_int),
@@ -283,6 +293,166 @@ def step(s: MHDState, dt: float, ch: Optional[float] = None, glm_cr: float = GLM
     T = np.float32
     decay = float(np.exp(T(T(-T(glm_cr) * T(ch) * T(dt)) / T(s.dx))))
     return step_cube(s, dt, ch, decay)
+
+
+# ---- source-coupled drag (lib/MHDKernels/src/drag.jl) ---------------------------------------
+
+def _target(v):
+    v = tuple(float(x) for x in v)
+    if len(v) != 3:
+        raise PMFMHDError("target_velocity must have three components")
+    return (ctypes.c_float * 3)(*v)
+
+
+def _check_impulse(q):
+    if not (np.isfinite(q) and q >= 0):
+        raise PMFMHDError("drag impulse must be finite and non-negative")
+
+
+def step_ref_drag(s: MHDState, dt: float, ch: float, decay: float, drag_impulse: float,
+                  target_velocity=(0.0, 0.0, 0.0)) -> MHDState:
+    """integrator_ref.jl:222-234: the fused step with the drag face prediction and the drag
+    corrector (CT states then run ct_update! without face compensation)."""
+    _check_impulse(drag_impulse)
+    v0 = _target(target_velocity)
+    if uses_ct(s):
+        _check(lib().pmfmhd_step_ct_drag(context(s.device), ctypes.byref(s.grid), _p9(s.U), _p9(s.scratch),
+                                         s.ct.packed.data_ptr(), float(dt), float(drag_impulse), v0, _stream()),
+               "step_ref_drag!")
+    else:
+        _check(lib().pmfmhd_step_glm_drag(context(s.device), ctypes.byref(s.grid), _p9(s.U), _p9(s.scratch),
+                                          float(dt), float(ch), float(decay), float(drag_impulse), v0, _stream()),
+               "step_ref_drag!")
+    s.U, s.scratch = s.scratch, s.U
+    return s
+
+
+def step_cube_drag(s: MHDState, dt: float, ch: float, decay: float, drag_impulse: float,
+                   target_velocity=(0.0, 0.0, 0.0)) -> MHDState:
+    """integrator_cube.jl:478-490: GLM states only, target at rest (the CMB frame). The
+    cubic-grid and N % 4 conditions of the reference's 4^3 cube do not apply to this kernel."""
+    if uses_ct(s):
+        raise PMFMHDError("step_cube_drag!: CT is implemented on the :ref integrator only "
+                          "(mhd_solver=:ct states cannot use the :cube integrators)")
+    if any(float(v) != 0.0 for v in target_velocity):
+        raise PMFMHDError("step_cube_drag! is specialized for Compton drag in the CMB frame; "
+                          "use integrator=:ref for a moving target")
+    return step_ref_drag(s, dt, ch, decay, drag_impulse)
+
+
+def step_drag_godunov(s: MHDState, dt: float, drag_impulse: float, ch: float, glm_cr: float = GLM_CR,
+                      integrator: str = "cube", target_velocity=(0.0, 0.0, 0.0)) -> MHDState:
+    """drag.jl:162-178: one source-aware Godunov step; decay = exp(-cr*ch*dt/dx) in FP32."""
+    _check_impulse(drag_impulse)
+    T = np.float32
+    decay = float(np.exp(T(T(-T(glm_cr) * T(ch) * T(dt)) / T(s.dx))))
+    if integrator == "ref":
+        return step_ref_drag(s, dt, ch, decay, drag_impulse, target_velocity)
+    if integrator == "cube":
+        return step_cube_drag(s, dt, ch, decay, drag_impulse, target_velocity)
+    raise PMFMHDError(f"unknown integrator :{integrator} (have :ref, :cube)")
+
+
+def apply_linear_drag(s: MHDState, decay: float, target_velocity=(0.0, 0.0, 0.0),
+                      energy_compensation: Optional[torch.Tensor] = None) -> MHDState:
+    """drag.jl:78-117: exact linear drag with velocity decay factor `decay` in [0, 1]."""
+    if not (np.isfinite(decay) and 0 <= decay <= 1):
+        raise PMFMHDError("linear drag decay must be finite and in [0,1]")
+    res = energy_compensation.data_ptr() if energy_compensation is not None else None
+    _check(lib().pmfmhd_apply_linear_drag(context(s.device), ctypes.byref(s.grid), _p9(s.U), float(decay),
+                                          _target(target_velocity), res, _stream()), "apply_linear_drag!")
+    return s
+
+
+def apply_exponential_drag_increment(s: MHDState, old_U, drag_impulse: float,
+                                     target_velocity=(0.0, 0.0, 0.0)) -> MHDState:
+    """drag.jl:121-208: exponential constant-force correction of the no-drag trial s.U."""
+    _check_impulse(drag_impulse)
+    if len(old_U) != NVAR:
+        raise PMFMHDError(f"old_U must contain {NVAR} conserved fields")
+    _check(lib().pmfmhd_apply_exponential_drag_increment(context(s.device), ctypes.byref(s.grid), _p9(s.U),
+                                                         _p9(old_U), float(drag_impulse), _target(target_velocity),
+                                                         _stream()), "apply_exponential_drag_increment!")
+    return s
+
+
+def step_drag_strang(s: MHDState, dt: float, drag_impulse: float, ch: Optional[float], glm_cr: float = 0.18,
+                     integrator: str = "cube", target_velocity=(0.0, 0.0, 0.0)) -> MHDState:
+    """drag.jl:218-228: exact half-step drag, one ideal-MHD step, exact half-step drag."""
+    _check_impulse(drag_impulse)
+    half_decay = float(np.exp(-0.5 * float(drag_impulse)))
+    apply_linear_drag(s, half_decay, target_velocity)
+    step(s, dt, ch=ch, glm_cr=glm_cr, integrator=integrator)
+    apply_linear_drag(s, half_decay, target_velocity)
+    return s
+
+
+def step_drag_exponential(s: MHDState, dt: float, drag_impulse: float, ch: Optional[float], glm_cr: float = 0.18,
+                          integrator: str = "cube", target_velocity=(0.0, 0.0, 0.0)) -> MHDState:
+    """drag.jl:240-250: a no-drag trial step, then the exponential increment against the
+    previous state (left in s.scratch by the ping-pong swap)."""
+    _check_impulse(drag_impulse)
+    step(s, dt, ch=ch, glm_cr=glm_cr, integrator=integrator)
+    return apply_exponential_drag_increment(s, s.scratch, drag_impulse, target_velocity)
+
+
+@dataclass
+class DragRegimeController:
+    """Hysteretic terminal / full-MHD regime switch (drag.jl:5-28)."""
+    exit_drag_over_omega: float = 1.0
+    enter_drag_over_omega: float = 2.0
+    min_va_over_cs: float = 0.0
+    confirm_checks: int = 2
+    reenter_terminal: bool = False
+    terminal: bool = False
+    initialized: bool = False
+    consecutive: int = 0
+
+    def __post_init__(self):
+        if not (0 < self.exit_drag_over_omega < self.enter_drag_over_omega):
+            raise PMFMHDError("drag regime hysteresis requires 0 < exit < enter")
+        if not self.min_va_over_cs >= 0:
+            raise PMFMHDError("min_va_over_cs must be non-negative")
+        if not self.confirm_checks >= 1:
+            raise PMFMHDError("confirm_checks must be positive")
+        self.exit_drag_over_omega = float(self.exit_drag_over_omega)
+        self.enter_drag_over_omega = float(self.enter_drag_over_omega)
+        self.min_va_over_cs = float(self.min_va_over_cs)
+        self.confirm_checks = int(self.confirm_checks)
+
+
+def update_drag_regime(controller: DragRegimeController, drag_over_omega: float, va_over_cs: float):
+    """drag.jl:38-76: one sampled check; returns (terminal, transition) with transition in
+    {"none", "terminal_to_full", "full_to_terminal"}. The handoff is one-way unless
+    ``reenter_terminal``; every switch needs ``confirm_checks`` consecutive votes."""
+    if not (np.isfinite(drag_over_omega) and drag_over_omega >= 0):
+        raise PMFMHDError("drag_over_omega must be finite and non-negative")
+    if not (np.isfinite(va_over_cs) and va_over_cs >= 0):
+        raise PMFMHDError("va_over_cs must be finite and non-negative")
+    c = controller
+    ratio, mag = float(drag_over_omega), float(va_over_cs)
+    if not c.initialized:
+        c.terminal = mag >= c.min_va_over_cs and ratio >= c.enter_drag_over_omega
+        c.initialized = True
+        c.consecutive = 0
+        return c.terminal, "none"
+    if c.terminal:
+        wants_full = mag < c.min_va_over_cs or ratio <= c.exit_drag_over_omega
+        c.consecutive = c.consecutive + 1 if wants_full else 0
+        if c.consecutive >= c.confirm_checks:
+            c.terminal = False
+            c.consecutive = 0
+            return False, "terminal_to_full"
+    elif c.reenter_terminal:
+        wants_terminal = mag >= c.min_va_over_cs and ratio >= c.enter_drag_over_omega
+        c.consecutive = c.consecutive + 1 if wants_terminal else 0
+        if c.consecutive >= c.confirm_checks:
+            c.terminal = True
+            c.consecutive = 0
+            return True, "full_to_terminal"
+    else:
+        c.consecutive = 0
+    return c.terminal, "none"
 
 
 def max_wavespeed(s: MHDState) -> float:
