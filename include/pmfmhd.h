@@ -116,6 +116,31 @@ int pmfmhd_step_glm_drag(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* con
 int pmfmhd_step_ct_drag(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],
                         float* ct_packed, float dt, float drag_impulse, const float target_velocity[3],
                         void* stream);
+/* Options of pmfmhd_step_radiation (bitwise or). */
+#define PMFMHD_RAD_TRACK_DENSITY 1         /* accumulate the density increments in slot 4 */
+#define PMFMHD_RAD_TRACK_MAGNETIC 2        /* Kahan-compensate cell B (GLM, slots 5-7) or the CT faces */
+#define PMFMHD_RAD_TRACK_ENERGY 4          /* Kahan-compensate E and the drag work (slot 8) */
+#define PMFMHD_RAD_CHECK_ADMISSIBILITY 8   /* write -max(|rho|, max(smallr, llf_dmin)) for rejected cells */
+#define PMFMHD_RAD_ROBUST_FALLBACK 16      /* minmod PLM with HLL on every face */
+#define PMFMHD_RAD_GLOBAL_FALLBACK 32      /* LLF on every face, with the admissibility check */
+/*
+ * Radiation-coupled step: the drag step (target at rest, impulse drag_impulse) whose face
+ * states also carry a per-cell velocity correction, with optional tracking of the density
+ * increment and Kahan remainders of E and B. Replaces `step_ref_radiation!`
+ * (integrator_ref.jl:238-258; GLM and CT) and `step_cube_radiation!`
+ * (integrator_cube.jl:504-540; check_admissibility, global_fallback and robust_fallback).
+ * `correction` is the caller's packed buffer of 9*nc floats, as the reference's
+ * `packed_psi_correction`: slot 0 holds psi and is read in place of U[8] (which may be
+ * null), slots 1-3 the velocity corrections added to every face state of their cell (and to
+ * the CT cell EMF velocity), slot 4 receives the density increments, slots 5-7 and 8 are
+ * the remainders of cell B (GLM) and E. For CT states (ct_packed non-null) ch and decay are
+ * ignored and the faces are compensated when PMFMHD_RAD_TRACK_MAGNETIC is set. Requires
+ * all-periodic boundaries. The masked per-face LLF fallback of the cube kernel
+ * (`fallback=true`, integrator_cube.jl:68-83) is not provided.
+ */
+int pmfmhd_step_radiation(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],
+                          float* ct_packed, float* correction, float dt, float ch, float decay, float drag_impulse,
+                          int flags, void* stream);
 /*
  * In-place exact linear drag with velocity decay factor `decay` in [0, 1]
  * (`apply_linear_drag!`, drag.jl:78-117): m <- rho v0 + (m - rho v0) decay with
@@ -177,6 +202,13 @@ int pmfmhd_conserved_totals_noalloc(const pmfmhd_grid* g, const float* const U[9
  */
 int pmfmhd_ct_faces_from_potential(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const A[3],
                                    float* const U[9], float* ct_packed, void* stream);
+/*
+ * Install the face field the caller wrote into ct_packed slots 0-2: face remainders zeroed,
+ * cell B = face average, E adjusted to keep the thermal pressure, psi = 0
+ * (`_ct_install_faces!`, ct.jl:222-236).
+ */
+int pmfmhd_ct_install_faces(pmfmhd_ctx* ctx, const pmfmhd_grid* g, float* const U[9], float* ct_packed,
+                            void* stream);
 
 /*
  * nsteps GLM steps with a fixed dt/ch/decay, ping-ponging between U and scratch, recorded

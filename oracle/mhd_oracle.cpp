@@ -305,9 +305,11 @@ template <class T> Q<T> drag_predict_face(const Q<T>& q0, const Q<T>& qh, T impu
   for (int c = 0; c < 3; ++c) r[1 + c] = v0[c] + decay * (q0[1 + c] - v0[c]) + phi1 * (qh[1 + c] - q0[1 + c]);
   return r;
 }
-// cell corrector: exact momentum response and integrated drag work (glm_physics.jl:128-172)
-template <class T> Q<T> drag_correct_conserved(const Q<T>& u0, const Q<T>& trial, T impulse, const T* v0, T smallr,
-                                               T smallE) {
+// cell corrector: exact momentum response and integrated drag work (glm_physics.jl:128-172);
+// the state with E still the trial's, the work qwork and the energy floor emin
+// (`_drag_correct_conserved_parts`)
+template <class T> Q<T> drag_correct_parts(const Q<T>& u0, const Q<T>& trial, T impulse, const T* v0, T smallr,
+                                           T smallE, T& qwork_out, T& emin_out) {
   T decay = std::exp(-impulse), phi1 = drag_phi1(impulse), A, C, D;
   drag_work_coefficients(impulse, A, C, D);
   T rn = mx(trial[0], smallr), ro = mx(u0[0], smallr);
@@ -327,8 +329,39 @@ template <class T> Q<T> drag_correct_conserved(const Q<T>& u0, const Q<T>& trial
   T nm[3] = {rn * vn[0], rn * vn[1], rn * vn[2]};
   T ek = T(0.5) * (nm[0] * nm[0] + nm[1] * nm[1] + nm[2] * nm[2]) / rn;
   T eb = T(0.5) * (trial[5] * trial[5] + trial[6] * trial[6] + trial[7] * trial[7]);
-  T emin = ek + eb + smallE;
-  return Q<T>{{rn, nm[0], nm[1], nm[2], mx(trial[4] - qwork, emin), trial[5], trial[6], trial[7], trial[8]}};
+  qwork_out = qwork;
+  emin_out = ek + eb + smallE;
+  return Q<T>{{rn, nm[0], nm[1], nm[2], trial[4], trial[5], trial[6], trial[7], trial[8]}};
+}
+template <class T> Q<T> drag_correct_conserved(const Q<T>& u0, const Q<T>& trial, T impulse, const T* v0, T smallr,
+                                               T smallE) {
+  T qwork, emin;
+  Q<T> r = drag_correct_parts(u0, trial, impulse, v0, smallr, smallE, qwork, emin);
+  r[4] = mx(trial[4] - qwork, emin);
+  return r;
+}
+
+// ---- radiation-coupled step flags (integrator_ref.jl:33-39,140-156; integrator_cube.jl:85-124) ----
+// corr is the packed 9*nc correction buffer: slot 0 is psi (read instead of U[8]), slots 1-3
+// the velocity corrections added to every face state, slot 4 the accumulated density
+// increment (track_density), slots 5-7 the Kahan remainders of cell B (track_magnetic,
+// GLM only) and slot 8 that of E (track_energy).
+enum { RAD_TRACK_DENSITY = 1, RAD_TRACK_MAGNETIC = 2, RAD_TRACK_ENERGY = 4, RAD_CHECK = 8 };
+template <class T> struct Rad {
+  T* corr;   // null: no radiation coupling
+  int flags;
+};
+// integrator_cube.jl:108-124
+template <class T> bool inadmissible(const Q<T>& r, const Phys<T>& P) {
+  T gate = mx(P.smallr, P.llf_dmin);
+  T ir = T(1) / mx(r[0], P.smallr);
+  T ek = T(0.5) * (r[1] * r[1] + r[2] * r[2] + r[3] * r[3]) * ir;
+  T eb = T(0.5) * (r[5] * r[5] + r[6] * r[6] + r[7] * r[7]);
+  T eint = r[4] - ek - eb;
+  T emin = P.pfl / (P.gamma - T(1));
+  bool finite = std::isfinite(r[0]) && std::isfinite(eint);
+  for (int v = 1; v < 9; ++v) finite = finite && std::isfinite(r[v]);
+  return !finite || r[0] < gate || eint < emin;
 }
 
 // CT workspace slots (ct.jl:71-93 consumer order; state.jl:44-52 names)
@@ -339,7 +372,7 @@ enum { W_MFX = 0, W_MFY, W_MFZ, W_FXBY, W_FXBZ, W_FYBX, W_FYBZ, W_FZBX, W_FZBY, 
 //   CT: faces (3nc, lower-face normal B) and work (W_N*nc) non-NULL.
 template <class T>
 void godunov(const Grid& g, const T* U, T* Un, T dtdx, T ch, T decay, const Phys<T>& P, T* resid,
-             const T* faces, T* work, const Drag<T>& drag) {
+             const T* faces, T* work, const Drag<T>& drag, const Rad<T>& rad = Rad<T>{nullptr, 0}) {
   const long nc = (long)g.nx * g.ny * g.nz;
   const bool CT = faces != nullptr;
 #pragma omp parallel for schedule(dynamic, 64)
@@ -351,12 +384,18 @@ void godunov(const Grid& g, const T* U, T* Un, T dtdx, T ch, T decay, const Phys
     for (int d = 0; d < 3; ++d) {
       Edges<T> em = mh_edges(g, U, nc, i - off[d][0], j - off[d][1], k - off[d][2], dtdx, P);
       Edges<T> ep = mh_edges(g, U, nc, i + off[d][0], j + off[d][1], k + off[d][2], dtdx, P);
-      // face states mh + offset, drag-propagated when drag is on (integrator_ref.jl:28-39)
-      auto face = [&](const Edges<T>& e, const Q<T>& off) {
-        return drag.on ? drag_predict_face(qadd(e.m0, off), qadd(e.mh, off), drag.qh, drag.v0) : qadd(e.mh, off);
+      // face states mh + offset, drag-propagated when drag is on, plus the radiation velocity
+      // correction of the owning cell (integrator_ref.jl:28-39)
+      auto face = [&](const Edges<T>& e, const Q<T>& off, long cell) {
+        Q<T> q = drag.on ? drag_predict_face(qadd(e.m0, off), qadd(e.mh, off), drag.qh, drag.v0) : qadd(e.mh, off);
+        if (rad.corr)
+          for (int v = 1; v <= 3; ++v) q[v] += rad.corr[v * nc + cell];
+        return q;
       };
-      Q<T> Ll = face(em, em.dR[d]), Rl = face(ec, ec.dL[d]);
-      Q<T> Lh = face(ec, ec.dR[d]), Rh = face(ep, ep.dL[d]);
+      const long cm = per(g, i - off[d][0], j - off[d][1], k - off[d][2]);
+      const long cp = per(g, i + off[d][0], j + off[d][1], k + off[d][2]);
+      Q<T> Ll = face(em, em.dR[d], cm), Rl = face(ec, ec.dL[d], c);
+      Q<T> Lh = face(ec, ec.dR[d], c), Rh = face(ep, ep.dL[d], cp);
       if (CT) {
         T bl = faces[d * nc + c];
         T bh = faces[d * nc + per(g, i + off[d][0], j + off[d][1], k + off[d][2])];
@@ -373,7 +412,9 @@ void godunov(const Grid& g, const T* U, T* Un, T dtdx, T ch, T decay, const Phys
       work[W_FYBX * nc + c] = Fl[1][5]; work[W_FYBZ * nc + c] = Fl[1][7];
       work[W_FZBX * nc + c] = Fl[2][5]; work[W_FZBY * nc + c] = Fl[2][6];
       const Q<T> qz{{T(0), T(0), T(0), T(0), T(0), T(0), T(0), T(0), T(0)}};
-      const Q<T> qc = drag.on ? drag_predict_face(qadd(ec.m0, qz), qadd(ec.mh, qz), drag.qh, drag.v0) : ec.mh;
+      Q<T> qc = drag.on ? drag_predict_face(qadd(ec.m0, qz), qadd(ec.mh, qz), drag.qh, drag.v0) : ec.mh;
+      if (rad.corr)
+        for (int v = 1; v <= 3; ++v) qc[v] += rad.corr[v * nc + c];
       work[W_ECX * nc + c] = qc[3] * U0[6] - qc[2] * U0[7];
       work[W_ECY * nc + c] = qc[1] * U0[7] - qc[3] * U0[5];
       work[W_ECZ * nc + c] = qc[2] * U0[5] - qc[1] * U0[6];
@@ -394,7 +435,32 @@ void godunov(const Grid& g, const T* U, T* Un, T dtdx, T ch, T decay, const Phys
       for (int v = 1; v < 8; ++v) r[v] = U0[v] + dU[v];
     }
     r[8] = U0[8] + dU[8];
-    if (drag.on) r = drag_correct_conserved(U0, r, drag.q, drag.v0, P.smallr, T(1e-30));  // integrator_ref.jl:155-156
+    bool bad = false;
+    if (rad.corr) {
+      // tracked density increment, compensated E and (GLM) cell B, admissibility flag
+      // (integrator_cube.jl:85-106,412-432)
+      T* cr = rad.corr;
+      if (rad.flags & RAD_TRACK_DENSITY) cr[4 * nc + c] += dU[0];
+      if (rad.flags & RAD_TRACK_ENERGY) r[4] = comp_update(cr, 8 * nc + c, U0[4], dU[4]);
+      if ((rad.flags & RAD_TRACK_MAGNETIC) && !CT)
+        for (int b = 0; b < 3; ++b) r[5 + b] = comp_update(cr, (5 + b) * nc + c, U0[5 + b], dU[5 + b]);
+      if (rad.flags & RAD_CHECK) bad = inadmissible(r, P);
+      // drag corrector, its work removed from E through the energy remainder when tracked
+      // (drag_correct_conserved_compensated!, glm_physics.jl:374-400; _compensated_floor_update!)
+      T qwork, emin;
+      const T e_trial = r[4];
+      r = drag_correct_parts(U0, r, drag.q, drag.v0, P.smallr, T(1e-30), qwork, emin);
+      if (rad.flags & RAD_TRACK_ENERGY) {
+        T e = comp_update(cr, 8 * nc + c, e_trial, -qwork);
+        if (e < emin) { cr[8 * nc + c] = T(0); e = emin; }
+        r[4] = e;
+      } else {
+        r[4] = mx(e_trial - qwork, emin);
+      }
+    } else if (drag.on) {
+      r = drag_correct_conserved(U0, r, drag.q, drag.v0, P.smallr, T(1e-30));  // integrator_ref.jl:155-156
+    }
+    if (bad) r[0] = -mx(std::fabs(r[0]), mx(P.smallr, P.llf_dmin));
     for (int v = 0; v < 8; ++v) Un[v * nc + c] = r[v];
     Un[8 * nc + c] = CT ? T(0) : r[8] * decay;
   }
@@ -576,6 +642,18 @@ struct oracle_params {
     Grid g = grid_##SUF(p);                                                                               \
     godunov<T>(g, U, Un, T(dtdx), T(0), T(1), phys_##SUF(p), resid, faces, work, no_drag_##SUF()); \
     ct_update<T>(g, Un, faces, work, face_resid, T(dtdx));                                                \
+  }                                                                                                        \
+  void oracle_step_glm_rad_##SUF(const oracle_params* p, const T* U, T* Un, double dtdx, double ch, double decay,  \
+                                 double q, T* corr, int flags) {                                          \
+    godunov<T>(grid_##SUF(p), U, Un, T(dtdx), T(ch), T(decay), phys_##SUF(p), nullptr, nullptr, nullptr,  \
+               drag_##SUF(q, nullptr), Rad<T>{corr, flags});                                               \
+  }                                                                                                        \
+  void oracle_step_ct_rad_##SUF(const oracle_params* p, const T* U, T* Un, T* faces, T* work, T* face_resid, \
+                                double dtdx, double q, T* corr, int flags) {                              \
+    Grid g = grid_##SUF(p);                                                                               \
+    godunov<T>(g, U, Un, T(dtdx), T(0), T(1), phys_##SUF(p), nullptr, faces, work, drag_##SUF(q, nullptr), \
+               Rad<T>{corr, flags});                                                                       \
+    ct_update<T>(g, Un, faces, work, (flags & RAD_TRACK_MAGNETIC) ? face_resid : nullptr, T(dtdx));       \
   }                                                                                                        \
   void oracle_step_ct_drag_##SUF(const oracle_params* p, const T* U, T* Un, T* faces, T* work, double dtdx, \
                                  double q, const double* v0) {                                            \

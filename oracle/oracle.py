@@ -53,6 +53,8 @@ def lib():
             getattr(_LIB, f"oracle_step_ct_{suf}").argtypes = [P, vp, vp, vp, vp, d, vp, vp]
             getattr(_LIB, f"oracle_step_glm_drag_{suf}").argtypes = [P, vp, vp, d, d, d, d, vp]
             getattr(_LIB, f"oracle_step_ct_drag_{suf}").argtypes = [P, vp, vp, vp, vp, d, d, vp]
+            getattr(_LIB, f"oracle_step_glm_rad_{suf}").argtypes = [P, vp, vp, d, d, d, d, vp, ctypes.c_int]
+            getattr(_LIB, f"oracle_step_ct_rad_{suf}").argtypes = [P, vp, vp, vp, vp, vp, d, d, vp, ctypes.c_int]
             for name in ("max_wavespeed",):
                 f = getattr(_LIB, f"oracle_{name}_{suf}")
                 f.argtypes = [P, vp]
@@ -130,6 +132,43 @@ class OracleState:
             decay = T(np.exp(T(-T(glm_cr) * T(ch) * T(dt) / self.dx)))
             self._f("step_glm_drag")(ctypes.byref(self.p), _ptr(self.U), _ptr(self.scratch), float(dtdx),
                                      float(T(ch)), float(decay), float(T(drag_impulse)), v0)
+        self.U, self.scratch = self.scratch, self.U
+
+    RAD_TRACK_DENSITY, RAD_TRACK_MAGNETIC, RAD_TRACK_ENERGY, RAD_CHECK = 1, 2, 4, 8
+
+    def step_radiation(self, dt, drag_impulse, correction, ch=0.0, decay=1.0, track_density=True,
+                       track_magnetic=True, track_energy=True, check_admissibility=False, robust_fallback=False,
+                       global_fallback=False):
+        """The radiation-coupled step kernel: step_ref_radiation! (integrator_ref.jl:238-258) and
+        step_cube_radiation! (integrator_cube.jl:504-540). ``correction`` is the packed (9, nc)
+        buffer of the state precision; its slot 0 is read as psi, slots 4-8 are updated.
+        robust_fallback: minmod PLM with HLL; global_fallback: LLF on every face (with the
+        admissibility flag)."""
+        T = self.T
+        corr = correction
+        assert corr.dtype == self.U.dtype and corr.shape == (9, self.nc) and corr.flags["C_CONTIGUOUS"]
+        flags = ((self.RAD_TRACK_DENSITY if track_density else 0) | (self.RAD_TRACK_MAGNETIC if track_magnetic else 0)
+                 | (self.RAD_TRACK_ENERGY if track_energy else 0)
+                 | (self.RAD_CHECK if (check_admissibility or global_fallback) else 0))
+        saved = (self.p.recon, self.p.riemann)
+        if robust_fallback:
+            self.p.recon, self.p.riemann = RECON["plm_minmod"], RIEMANN["hll"]
+        elif global_fallback:
+            self.p.riemann = RIEMANN["llf"]
+        Uin = np.concatenate([self.U[:8], corr[:1]])
+        dtdx = T(T(dt) / self.dx)
+        try:
+            if self.mhd_solver == "ct":
+                if self.face_resid is None:
+                    self.face_resid = np.zeros((3, self.nc), dtype=self.U.dtype)
+                self._f("step_ct_rad")(ctypes.byref(self.p), _ptr(Uin), _ptr(self.scratch), _ptr(self.faces),
+                                       _ptr(self.work), _ptr(self.face_resid), float(dtdx), float(T(drag_impulse)),
+                                       _ptr(corr), flags)
+            else:
+                self._f("step_glm_rad")(ctypes.byref(self.p), _ptr(Uin), _ptr(self.scratch), float(dtdx),
+                                        float(T(ch)), float(T(decay)), float(T(drag_impulse)), _ptr(corr), flags)
+        finally:
+            self.p.recon, self.p.riemann = saved
         self.U, self.scratch = self.scratch, self.U
 
     def _drag_phi1(self, q):

@@ -158,8 +158,8 @@ int occupancy_of(const StepKernelInfo& k) {
 }
 
 int launch_step(pmfmhd_ctx* c, const pmfmhd_grid* g, StepArgs& a, Tune t, bool ct, bool comp,
-                cudaStream_t s, bool drag = false) {
-  StepKernelInfo k = step_kernel_info(t.ty, g->recon, g->riemann, ct, comp, drag);
+                cudaStream_t s, int src = SRC_NONE) {
+  StepKernelInfo k = step_kernel_info(t.ty, g->recon, g->riemann, ct, comp, src);
   if (k.fn == nullptr) return PMFMHD_EUNSUPPORTED;
   const int occ = occupancy_of(k);
   a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
@@ -215,26 +215,41 @@ DragCoef drag_coefficients(float q, const float* v0) {
   return k;
 }
 
+// Source terms of a source-coupled step: drag, or radiation coupling (drag + corrections).
+struct SourceTerms {
+  int src = SRC_NONE;
+  DragCoef drag{};
+  float* corr = nullptr;
+  int rad_flags = 0;
+};
+
+void apply_sources(StepArgs& a, const SourceTerms* st) {
+  if (st == nullptr) return;
+  a.drag = st->drag;
+  a.corr = st->corr;
+  a.rad_flags = st->rad_flags;
+}
+
 int enqueue_glm(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Un[9], float dt,
-                float ch, float decay, float* const resid[7], bool comp, cudaStream_t s, const DragCoef* drag) {
+                float ch, float decay, float* const resid[7], bool comp, cudaStream_t s, const SourceTerms* st) {
   StepArgs a;
   const float dtdx = dt / g->dx;  // T(dt)/s.dx (integrator_ref.jl:211)
   fill_glm_args(a, U, Un, resid, comp, dtdx, ch, decay, c->d_smax);
-  if (drag) a.drag = *drag;
+  apply_sources(a, st);
   PMF_CK(cudaMemsetAsync(c->d_smax, 0, sizeof(unsigned int), s));
-  return launch_step(c, g, a, tune_for(c, g, false, comp), false, comp, s, drag != nullptr);
+  return launch_step(c, g, a, tune_for(c, g, false, comp), false, comp, s, st ? st->src : SRC_NONE);
 }
 
 int enqueue_ct(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Un[9], float* ct, float dt,
-               float* const resid[7], bool comp, bool comp_faces, cudaStream_t s, const DragCoef* drag) {
+               float* const resid[7], bool comp, bool comp_faces, cudaStream_t s, const SourceTerms* st) {
   const long long nc = ncells(g);
   const float dtdx = dt / g->dx;
   StepArgs a;
   fill_glm_args(a, U, Un, resid, comp, dtdx, 0.0f, 1.0f, nullptr);
-  if (drag) a.drag = *drag;
+  apply_sources(a, st);
   for (int d = 0; d < 3; ++d) a.face[d] = ct + (size_t)(CT_BXF + d) * nc;
   for (int k = 0; k < CT_NWORK; ++k) a.work[k] = ct + (size_t)(CT_MFX + k) * nc;
-  int rc = launch_step(c, g, a, tune_for(c, g, true, comp), true, comp, s, drag != nullptr);
+  int rc = launch_step(c, g, a, tune_for(c, g, true, comp), true, comp, s, st ? st->src : SRC_NONE);
   if (rc != PMFMHD_OK) return rc;
   const int nb = aux_blocks(c, nc);
   ct_emf_kernel<<<nb, AUX_THREADS, 0, s>>>(ct, g->nx, g->ny, g->nz);
@@ -353,8 +368,10 @@ int pmfmhd_step_glm_drag(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const
   if (!nonnull(U, 9) || !nonnull(Unew, 9)) return PMFMHD_EINVAL;
   if (!std::isfinite(dt) || !std::isfinite(ch) || !std::isfinite(decay) || !(ch > 0.0f)) return PMFMHD_EINVAL;
   if (!std::isfinite(drag_impulse) || !(drag_impulse >= 0.0f)) return PMFMHD_EINVAL;
-  const DragCoef k = drag_coefficients(drag_impulse, target_velocity);
-  return enqueue_glm(c, g, U, Unew, dt, ch, decay, nullptr, false, as_stream(stream), &k);
+  SourceTerms st;
+  st.src = SRC_DRAG;
+  st.drag = drag_coefficients(drag_impulse, target_velocity);
+  return enqueue_glm(c, g, U, Unew, dt, ch, decay, nullptr, false, as_stream(stream), &st);
 }
 
 int pmfmhd_step_ct_drag(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],
@@ -367,8 +384,53 @@ int pmfmhd_step_ct_drag(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const 
   if (!nonnull(U, 9) || !nonnull(Unew, 9)) return PMFMHD_EINVAL;
   if (!std::isfinite(dt)) return PMFMHD_EINVAL;
   if (!std::isfinite(drag_impulse) || !(drag_impulse >= 0.0f)) return PMFMHD_EINVAL;
-  const DragCoef k = drag_coefficients(drag_impulse, target_velocity);
-  return enqueue_ct(c, g, U, Unew, ct_packed, dt, nullptr, false, false, as_stream(stream), &k);
+  SourceTerms st;
+  st.src = SRC_DRAG;
+  st.drag = drag_coefficients(drag_impulse, target_velocity);
+  return enqueue_ct(c, g, U, Unew, ct_packed, dt, nullptr, false, false, as_stream(stream), &st);
+}
+
+int pmfmhd_step_radiation(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],
+                          float* ct_packed, float* correction, float dt, float ch, float decay, float drag_impulse,
+                          int flags, void* stream) {
+  if (c == nullptr || correction == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!all_periodic(g)) return PMFMHD_EUNSUPPORTED;
+  for (int f = 0; f < 8; ++f)
+    if (U[f] == nullptr) return PMFMHD_EINVAL;
+  if (!nonnull(Unew, 9)) return PMFMHD_EINVAL;
+  if (flags & ~(PMFMHD_RAD_TRACK_DENSITY | PMFMHD_RAD_TRACK_MAGNETIC | PMFMHD_RAD_TRACK_ENERGY |
+                PMFMHD_RAD_CHECK_ADMISSIBILITY | PMFMHD_RAD_ROBUST_FALLBACK | PMFMHD_RAD_GLOBAL_FALLBACK))
+    return PMFMHD_EINVAL;
+  if (!std::isfinite(dt) || !std::isfinite(drag_impulse) || !(drag_impulse >= 0.0f)) return PMFMHD_EINVAL;
+  const bool ct = ct_packed != nullptr;
+  if (!ct && (!std::isfinite(ch) || !std::isfinite(decay) || !(ch > 0.0f))) return PMFMHD_EINVAL;
+  // fallback steps swap the scheme without touching the caller's recon/riemann choice
+  // (integrator_ref.jl:243-246, integrator_cube.jl:524-529)
+  pmfmhd_grid g2 = *g;
+  int rf = flags & (RAD_TRACK_DENSITY | RAD_TRACK_MAGNETIC | RAD_TRACK_ENERGY | RAD_CHECK);
+  if (flags & PMFMHD_RAD_ROBUST_FALLBACK) {
+    g2.recon = PMFMHD_RECON_PLM_MINMOD;
+    g2.riemann = PMFMHD_RIEMANN_HLL;
+  } else if (flags & PMFMHD_RAD_GLOBAL_FALLBACK) {
+    g2.riemann = PMFMHD_RIEMANN_LLF;
+    rf |= RAD_CHECK;
+  }
+  // psi is read from slot 0 of the correction buffer, as the reference passes the buffer in
+  // place of U[9]
+  const float* Uin[9];
+  for (int f = 0; f < 8; ++f) Uin[f] = U[f];
+  Uin[8] = correction;
+  SourceTerms st;
+  st.src = SRC_RAD;
+  st.drag = drag_coefficients(drag_impulse, nullptr);
+  st.corr = correction;
+  st.rad_flags = rf;
+  if (ct)
+    return enqueue_ct(c, &g2, Uin, Unew, ct_packed, dt, nullptr, false, (rf & RAD_TRACK_MAGNETIC) != 0,
+                      as_stream(stream), &st);
+  return enqueue_glm(c, &g2, Uin, Unew, dt, ch, decay, nullptr, false, as_stream(stream), &st);
 }
 
 int pmfmhd_max_wavespeed(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* smax, void* stream) {
@@ -465,9 +527,22 @@ int pmfmhd_ct_faces_from_potential(pmfmhd_ctx* c, const pmfmhd_grid* g, const fl
   cudaStream_t s = as_stream(stream);
   const int nb = aux_blocks(c, ncells(g));
   ct_curl_kernel<<<nb, AUX_THREADS, 0, s>>>(A[0], A[1], A[2], ct, g->nx, g->ny, g->nz, 1.0f / g->dx);
+  PMF_CK(cudaGetLastError());
+  return pmfmhd_ct_install_faces(c, g, U, ct, stream);
+}
+
+int pmfmhd_ct_install_faces(pmfmhd_ctx* c, const pmfmhd_grid* g, float* const U[9], float* ct, void* stream) {
+  if (c == nullptr || ct == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!all_periodic(g)) return PMFMHD_EUNSUPPORTED;
+  if (!nonnull(U, 9)) return PMFMHD_EINVAL;
+  cudaStream_t s = as_stream(stream);
+  const long long nc = ncells(g);
+  PMF_CK(cudaMemsetAsync(ct + (size_t)CT_RBX * nc, 0, sizeof(float) * 3 * (size_t)nc, s));
   MPtr9 u;
   for (int f = 0; f < 9; ++f) u.p[f] = U[f];
-  ct_cell_from_faces_kernel<<<nb, AUX_THREADS, 0, s>>>(ct, u, g->nx, g->ny, g->nz);
+  ct_cell_from_faces_kernel<<<aux_blocks(c, nc), AUX_THREADS, 0, s>>>(ct, u, g->nx, g->ny, g->nz);
   PMF_CK(cudaGetLastError());
   return PMFMHD_OK;
 }

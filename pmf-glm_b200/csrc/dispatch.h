@@ -18,8 +18,8 @@ struct StepKernelInfo {
 constexpr int kTileRows[] = {5, 8, 10, 13};
 constexpr int kNumTileRows = 4;
 
-// `drag`: the source-coupled drag step (uncompensated; `comp` must be false).
-StepKernelInfo step_kernel_info(int ty, int recon, int rsol, bool ct, bool comp, bool drag = false);
+// `src`: SRC_NONE, or a source-coupled step (SRC_DRAG, SRC_RAD; `comp` must be false).
+StepKernelInfo step_kernel_info(int ty, int recon, int rsol, bool ct, bool comp, int src = 0);
 // The many-box form of the same kernel (same shared memory and block size).
 BatchKernel batch_kernel(int ty, int recon, int rsol, bool ct, bool comp);
 }  // namespace pmf

@@ -416,6 +416,13 @@ __device__ __forceinline__ float cell_wavespeed(const F9& u, const Phys& P) {
 
 // Kahan-compensated accumulation with a persistent remainder (glm_physics.jl:349-359).
 // The fast-math build must not reassociate it, so the rounding steps are explicit.
+__device__ __forceinline__ float comp_add(float x, float dx, float& r) {
+  float inc = __fadd_rn(dx, r);
+  float upd = __fadd_rn(x, inc);
+  r = __fsub_rn(inc, __fsub_rn(upd, x));
+  return upd;
+}
+
 // ---- linear (Compton) drag toward a target velocity, glm_physics.jl:63-172 ------------------
 // Coefficients of one step with impulse q = Gamma*dt (computed on the host in FP32 with the
 // reference's formulas): the face prediction uses the half-step pair (exp(-q/2), phi1(q/2)),
@@ -451,8 +458,12 @@ __device__ __forceinline__ void drag_predict_cell(F9& mh, const F9& m0, Offsets<
 
 // Cell corrector (glm_physics.jl:128-172): exact momentum response to the trial velocity
 // increment and the analytically integrated drag work removed from E, with the density
-// floored at smallr and E floored at the new kinetic + magnetic energy + 1e-30.
-__device__ __forceinline__ void drag_correct_cell(const F9& u0, F9& t, const DragCoef& k, float smallr) {
+// floored at smallr and E floored at the new kinetic + magnetic energy + 1e-30. With `rE`
+// the work is removed through E's Kahan remainder, which is cleared when the floor applies
+// (drag_correct_conserved_compensated!, glm_physics.jl:374-400 with
+// _compensated_floor_update!, :361-372).
+__device__ __forceinline__ void drag_correct_cell(const F9& u0, F9& t, const DragCoef& k, float smallr,
+                                                  float* rE = nullptr) {
   const float rn = fmaxf(t[0], smallr), ro = fmaxf(u0[0], smallr);
   float w[3], dv[3], vn[3], iw[3];
 #pragma unroll
@@ -475,15 +486,32 @@ __device__ __forceinline__ void drag_correct_cell(const F9& u0, F9& t, const Dra
   t[1] = nm0;
   t[2] = nm1;
   t[3] = nm2;
-  t[4] = fmaxf(t[4] - qwork, ek + eb + 1e-30f);
+  const float emin = ek + eb + 1e-30f;
+  if (rE == nullptr) {
+    t[4] = fmaxf(t[4] - qwork, emin);
+  } else {
+    float e = comp_add(t[4], -qwork, *rE);
+    if (e < emin) {
+      *rE = 0.0f;
+      e = emin;
+    }
+    t[4] = e;
+  }
 }
 
-__device__ __forceinline__ float comp_add(float x, float dx, float& r) {
-  float inc = __fadd_rn(dx, r);
-  float upd = __fadd_rn(x, inc);
-  r = __fsub_rn(inc, __fsub_rn(upd, x));
-  return upd;
+// Admissibility of a trial conserved state (integrator_cube.jl:108-124): finite, density
+// at least max(smallr, llf_dmin) and internal energy at least pfl/(gamma-1).
+__device__ __forceinline__ bool inadmissible_cell(const F9& r, const Phys& P) {
+  const float ir = 1.0f / fmaxf(r[0], P.smallr);
+  const float ek = 0.5f * (r[1] * r[1] + r[2] * r[2] + r[3] * r[3]) * ir;
+  const float eb = 0.5f * (r[5] * r[5] + r[6] * r[6] + r[7] * r[7]);
+  const float eint = r[4] - ek - eb;
+  bool finite = isfinite(eint);
+#pragma unroll
+  for (int v = 0; v < 9; ++v) finite = finite && isfinite(r[v]);
+  return !finite || r[0] < fmaxf(P.smallr, P.llf_dmin) || eint < P.pfl / (P.gamma - 1.0f);
 }
+
 
 // BC index map for a logical cell index (boundary.jl:161-175, 0-based): returns the source
 // index; *flip = -1 where a reflecting wall mirrors the normal vector components.

@@ -2,10 +2,10 @@
 #include "dispatch.h"
 
 namespace pmf {
-StepKernelInfo step_kernel_info_ty5(int recon, int rsol, bool ct, bool comp, bool drag);
-StepKernelInfo step_kernel_info_ty8(int recon, int rsol, bool ct, bool comp, bool drag);
-StepKernelInfo step_kernel_info_ty10(int recon, int rsol, bool ct, bool comp, bool drag);
-StepKernelInfo step_kernel_info_ty13(int recon, int rsol, bool ct, bool comp, bool drag);
+StepKernelInfo step_kernel_info_ty5(int recon, int rsol, bool ct, bool comp, int src);
+StepKernelInfo step_kernel_info_ty8(int recon, int rsol, bool ct, bool comp, int src);
+StepKernelInfo step_kernel_info_ty10(int recon, int rsol, bool ct, bool comp, int src);
+StepKernelInfo step_kernel_info_ty13(int recon, int rsol, bool ct, bool comp, int src);
 
 BatchKernel batch_kernel_ty5(int recon, int rsol, bool ct, bool comp);
 BatchKernel batch_kernel_ty8(int recon, int rsol, bool ct, bool comp);
@@ -22,12 +22,12 @@ BatchKernel batch_kernel(int ty, int recon, int rsol, bool ct, bool comp) {
   return nullptr;
 }
 
-StepKernelInfo step_kernel_info(int ty, int recon, int rsol, bool ct, bool comp, bool drag) {
+StepKernelInfo step_kernel_info(int ty, int recon, int rsol, bool ct, bool comp, int src) {
   switch (ty) {
-    case 5: return step_kernel_info_ty5(recon, rsol, ct, comp, drag);
-    case 8: return step_kernel_info_ty8(recon, rsol, ct, comp, drag);
-    case 10: return step_kernel_info_ty10(recon, rsol, ct, comp, drag);
-    case 13: return step_kernel_info_ty13(recon, rsol, ct, comp, drag);
+    case 5: return step_kernel_info_ty5(recon, rsol, ct, comp, src);
+    case 8: return step_kernel_info_ty8(recon, rsol, ct, comp, src);
+    case 10: return step_kernel_info_ty10(recon, rsol, ct, comp, src);
+    case 13: return step_kernel_info_ty13(recon, rsol, ct, comp, src);
   }
   return StepKernelInfo{nullptr, 0, 0};
 }

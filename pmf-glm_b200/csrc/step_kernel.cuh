@@ -55,8 +55,16 @@ struct StepArgs {
   unsigned int* status;     // device status bits (1: a bounded wait for a TMA load gave up), or null
   int use_tma;              // the tensor maps below describe U (fields with nx % 4 == 0)
   CUtensorMap tmap[9];      // per field: 3-D (x, y, z) FP32 map, box (PLANE_W, TY+4, 1)
-  DragCoef drag;            // source-coupled drag step: coefficients (read only by DRAG kernels)
+  DragCoef drag;            // source-coupled steps: drag coefficients (read by SRC_DRAG/SRC_RAD kernels)
+  float* corr;              // SRC_RAD: packed 9*nc correction buffer (slot 0 psi, 1-3 velocity
+                            // corrections, 4 density increments, 5-7 B / 8 E remainders)
+  int rad_flags;            // SRC_RAD: RAD_* bits
 };
+
+// Source terms of the step (template parameter SRC of the step kernel).
+enum { SRC_NONE = 0, SRC_DRAG = 1, SRC_RAD = 2 };
+// Runtime options of the radiation-coupled step (StepArgs::rad_flags).
+enum { RAD_TRACK_DENSITY = 1, RAD_TRACK_MAGNETIC = 2, RAD_TRACK_ENERGY = 4, RAD_CHECK = 8 };
 
 template <int TY>
 struct StepSmem {
@@ -85,11 +93,13 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // One column segment: planes [z0, z1) of column tile (tx, ty) of the box described by `a`.
 // Every thread of the CTA calls it; `smax` accumulates the new state's max signal speed.
-template <int TY, int RECON, int RSOL, bool CT, bool COMP, bool DRAG>
+template <int TY, int RECON, int RSOL, bool CT, bool COMP, int SRC>
 __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, int z0, int z1, float* smem,
                                              float& smax, unsigned long long* tma_bar, unsigned& tma_phase,
                                              int* tma_off) {
-  static_assert(!(DRAG && COMP), "the drag step updates without compensation");
+  constexpr bool DRAG = SRC != SRC_NONE;  // the radiation-coupled step always carries drag
+  constexpr bool RAD = SRC == SRC_RAD;
+  static_assert(!(DRAG && COMP), "source-coupled steps use their own remainders");
   using S = StepSmem<TY>;
   constexpr int NT = step_threads<TY>();
   constexpr int PP = S::PP;
@@ -276,6 +286,10 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   const int r0 = halo_warp ? (halo_act ? hrow + 2 : 2) : w + 1;
   const int c0 = halo_warp ? (hside ? PLANE_X0 + TILE_X : PLANE_X0 - 1) : PLANE_X0 + lane;
 
+  // radiation: in-plane offset of this thread's cell, wrapped periodically (halo cells and
+  // the columns/rows of a partial tile beyond the grid are periodic images)
+  const int rad_xy = RAD ? (((y % ny) + ny) % ny) * nx + ((x % nx) + nx) % nx : 0;
+
   // Conservative update of cell (x, y, pz) from its x/y divergence and its two z fluxes.
   auto update_cell = [&](int pz, const F9& dxy, const F9& flo, const F9& fhi) {
     const int c = pz * nxy + y * nx + x;
@@ -306,9 +320,35 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
 #pragma unroll
       for (int i = 1; i <= 7; ++i) un[i] = u0[i] + d[i];
     }
-    // drag corrector on the uncompensated trial (its energy floor reads the trial cell B,
-    // which CT later replaces by the face average); integrator_ref.jl:155-156
-    if constexpr (DRAG) drag_correct_cell(u0, un, a.drag, P.smallr);
+    if constexpr (RAD) {
+      // radiation-coupled update (integrator_cube.jl:85-106,412-436; integrator_ref.jl:140-156):
+      // density increment accumulated, E and (GLM) cell B through their Kahan remainders,
+      // admissibility flag, drag corrector with E's remainder; negative density marks a
+      // rejected cell
+      const size_t n = (size_t)nxy * nz, cc = (size_t)c;
+      const int fl = a.rad_flags;
+      float* cr = a.corr;
+      if (fl & RAD_TRACK_DENSITY) cr[4 * n + cc] += d[0];
+      float rE = (fl & RAD_TRACK_ENERGY) ? cr[8 * n + cc] : 0.0f;
+      if (fl & RAD_TRACK_ENERGY) un[4] = comp_add(u0[4], d[4], rE);
+      if (!CT && (fl & RAD_TRACK_MAGNETIC)) {
+#pragma unroll
+        for (int i = 5; i <= 7; ++i) {
+          float r = cr[(size_t)i * n + cc];
+          un[i] = comp_add(u0[i], d[i], r);
+          cr[(size_t)i * n + cc] = r;
+        }
+      }
+      un[8] = u0[8] + d[8];
+      const bool bad = (fl & RAD_CHECK) && inadmissible_cell(un, P);
+      drag_correct_cell(u0, un, a.drag, P.smallr, (fl & RAD_TRACK_ENERGY) ? &rE : nullptr);
+      if (fl & RAD_TRACK_ENERGY) cr[8 * n + cc] = rE;
+      if (bad) un[0] = -fmaxf(fabsf(un[0]), fmaxf(P.smallr, P.llf_dmin));
+    } else if constexpr (DRAG) {
+      // drag corrector on the uncompensated trial (its energy floor reads the trial cell B,
+      // which CT later replaces by the face average); integrator_ref.jl:155-156
+      drag_correct_cell(u0, un, a.drag, P.smallr);
+    }
     un[8] = CT ? 0.0f : (u0[8] + d[8]) * decay;
 #pragma unroll
     for (int f = 0; f < 9; ++f) {
@@ -368,6 +408,17 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     // drag: face states and the CT cell EMF see the drag-propagated velocity
     // (integrator_ref.jl:28-31,135)
     if constexpr (DRAG) drag_predict_cell<RECON>(mh, m0, ox, oy, oz, a.drag);
+    // radiation: the cell's velocity correction is added to all its face states and to the
+    // CT cell EMF velocity (integrator_ref.jl:33-39,135); its periodic image for halo cells
+    if constexpr (RAD) {
+      if (!halo_warp || halo_act) {
+        const size_t n = (size_t)nxy * nz;
+        const size_t gi = (size_t)wrap1(p, nz) * nxy + rad_xy;
+        mh[1] += __ldg(a.corr + n + gi);
+        mh[2] += __ldg(a.corr + 2 * n + gi);
+        mh[3] += __ldg(a.corr + 3 * n + gi);
+      }
+    }
     if constexpr (CT) {
       // cell-centred reference EMF -v x B: v of the predicted state, B at the start of the
       // step (integrator_ref.jl:133-138)
@@ -541,7 +592,7 @@ __device__ __forceinline__ void cta_range(long long Q, long long* q0, long long*
 }
 
 // One box: a persistent launch of one CTA per resident slot.
-template <int TY, int RECON, int RSOL, bool CT, bool COMP, bool DRAG>
+template <int TY, int RECON, int RSOL, bool CT, bool COMP, int SRC>
 __global__ void __launch_bounds__(step_threads<TY>(), 1) mhd_step_kernel(const __grid_constant__ StepArgs a) {
   extern __shared__ __align__(128) float smem[];
   __shared__ unsigned long long tma_bar;
@@ -555,7 +606,7 @@ __global__ void __launch_bounds__(step_threads<TY>(), 1) mhd_step_kernel(const _
     const int col = (int)(q / a.nz);
     const int z0 = (int)(q - (long long)col * a.nz);
     const int z1 = (int)min((long long)a.nz, z0 + (qe - q));
-    march_column<TY, RECON, RSOL, CT, COMP, DRAG>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar,
+    march_column<TY, RECON, RSOL, CT, COMP, SRC>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar,
                                                   tma_phase, &tma_off);
     q += z1 - z0;
   }
@@ -598,7 +649,7 @@ __global__ void __launch_bounds__(step_threads<TY>(), 1) mhd_batch_kernel(const 
     const int col = (int)(local / a.nz);
     const int z0 = (int)(local - (long long)col * a.nz);
     const int z1 = (int)min((long long)a.nz, z0 + (qe - q));
-    march_column<TY, RECON, RSOL, CT, COMP, false>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar,
+    march_column<TY, RECON, RSOL, CT, COMP, SRC_NONE>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar,
                                                    tma_phase, &tma_off);
     q += z1 - z0;
   }

@@ -6,11 +6,16 @@
 namespace pmf {
 namespace detail {
 template <int TY, int RECON, int RSOL>
-StepKernel pick(bool ct, bool comp, bool drag) {
-  if (drag) return ct ? mhd_step_kernel<TY, RECON, RSOL, true, false, true> : mhd_step_kernel<TY, RECON, RSOL, false, false, true>;
+StepKernel pick(bool ct, bool comp, int src) {
+  if (src == SRC_DRAG)
+    return ct ? mhd_step_kernel<TY, RECON, RSOL, true, false, SRC_DRAG> : mhd_step_kernel<TY, RECON, RSOL, false, false, SRC_DRAG>;
+  if (src == SRC_RAD)
+    return ct ? mhd_step_kernel<TY, RECON, RSOL, true, false, SRC_RAD> : mhd_step_kernel<TY, RECON, RSOL, false, false, SRC_RAD>;
   if (ct)
-    return comp ? mhd_step_kernel<TY, RECON, RSOL, true, true, false> : mhd_step_kernel<TY, RECON, RSOL, true, false, false>;
-  return comp ? mhd_step_kernel<TY, RECON, RSOL, false, true, false> : mhd_step_kernel<TY, RECON, RSOL, false, false, false>;
+    return comp ? mhd_step_kernel<TY, RECON, RSOL, true, true, SRC_NONE>
+                : mhd_step_kernel<TY, RECON, RSOL, true, false, SRC_NONE>;
+  return comp ? mhd_step_kernel<TY, RECON, RSOL, false, true, SRC_NONE>
+              : mhd_step_kernel<TY, RECON, RSOL, false, false, SRC_NONE>;
 }
 template <int TY, int RECON, int RSOL>
 BatchKernel pick_batch(bool ct, bool comp) {
@@ -36,21 +41,21 @@ BatchKernel batch(int recon, int rsol, bool ct, bool comp) {
   return nullptr;
 }
 template <int TY, int RECON>
-StepKernel pick_rs(int rsol, bool ct, bool comp, bool drag) {
+StepKernel pick_rs(int rsol, bool ct, bool comp, int src) {
   switch (rsol) {
-    case RS_HLLD: return pick<TY, RECON, RS_HLLD>(ct, comp, drag);
-    case RS_HLL: return pick<TY, RECON, RS_HLL>(ct, comp, drag);
-    case RS_LLF: return pick<TY, RECON, RS_LLF>(ct, comp, drag);
+    case RS_HLLD: return pick<TY, RECON, RS_HLLD>(ct, comp, src);
+    case RS_HLL: return pick<TY, RECON, RS_HLL>(ct, comp, src);
+    case RS_LLF: return pick<TY, RECON, RS_LLF>(ct, comp, src);
   }
   return nullptr;
 }
 template <int TY>
-StepKernelInfo info(int recon, int rsol, bool ct, bool comp, bool drag) {
+StepKernelInfo info(int recon, int rsol, bool ct, bool comp, int src) {
   StepKernelInfo k{nullptr, StepSmem<TY>::BYTES, step_threads<TY>()};
   switch (recon) {
-    case RECON_PLM: k.fn = pick_rs<TY, RECON_PLM>(rsol, ct, comp, drag); break;
-    case RECON_PPM: k.fn = pick_rs<TY, RECON_PPM>(rsol, ct, comp, drag); break;
-    case RECON_PLM_MINMOD: k.fn = pick_rs<TY, RECON_PLM_MINMOD>(rsol, ct, comp, drag); break;
+    case RECON_PLM: k.fn = pick_rs<TY, RECON_PLM>(rsol, ct, comp, src); break;
+    case RECON_PPM: k.fn = pick_rs<TY, RECON_PPM>(rsol, ct, comp, src); break;
+    case RECON_PLM_MINMOD: k.fn = pick_rs<TY, RECON_PLM_MINMOD>(rsol, ct, comp, src); break;
   }
   return k;
 }

@@ -2,8 +2,8 @@
 #include "step_pick.cuh"
 
 namespace pmf {
-StepKernelInfo step_kernel_info_ty8(int recon, int rsol, bool ct, bool comp, bool drag) {
-  return detail::info<8>(recon, rsol, ct, comp, drag);
+StepKernelInfo step_kernel_info_ty8(int recon, int rsol, bool ct, bool comp, int src) {
+  return detail::info<8>(recon, rsol, ct, comp, src);
 }
 BatchKernel batch_kernel_ty8(int recon, int rsol, bool ct, bool comp) {
   return detail::batch<8>(recon, rsol, ct, comp);

@@ -70,6 +70,9 @@ SIGNATURES = {
     "pmfmhd_step_glm_drag": ([_VP, _GP, _P9, _P9, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                               _F3P, _VP], ctypes.c_int),
     "pmfmhd_step_ct_drag": ([_VP, _GP, _P9, _P9, _VP, ctypes.c_float, ctypes.c_float, _F3P, _VP], ctypes.c_int),
+    "pmfmhd_step_radiation": ([_VP, _GP, _P9, _P9, _VP, _VP, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                               ctypes.c_float, ctypes.c_int, _VP], ctypes.c_int),
+    "pmfmhd_ct_install_faces": ([_VP, _GP, _P9, _VP, _VP], ctypes.c_int),
     "pmfmhd_apply_linear_drag": ([_VP, _GP, _P9, ctypes.c_float, _F3P, _VP, _VP], ctypes.c_int),
     "pmfmhd_apply_exponential_drag_increment": ([_VP, _GP, _P9, _P9, ctypes.c_float, _F3P, _VP], ctypes.c_int),
     "pmfmhd_max_wavespeed": ([_VP, _GP, _P9, ctypes.POINTER(ctypes.c_float), _VP], ctypes.c_int),
@@ -353,6 +356,60 @@ def step_drag_godunov(s: MHDState, dt: float, drag_impulse: float, ch: float, gl
     raise PMFMHDError(f"unknown integrator :{integrator} (have :ref, :cube)")
 
 
+RAD_TRACK_DENSITY, RAD_TRACK_MAGNETIC, RAD_TRACK_ENERGY = 1, 2, 4
+RAD_CHECK_ADMISSIBILITY, RAD_ROBUST_FALLBACK, RAD_GLOBAL_FALLBACK = 8, 16, 32
+
+
+def allocate_radiation_correction(s: MHDState) -> torch.Tensor:
+    """A zeroed packed correction buffer (9*nc floats) with slot 0 set to the state's psi,
+    the layout of the reference's ``packed_psi_correction`` (radiation_coupling.jl:207-214)."""
+    corr = torch.zeros(9 * s.nc, dtype=torch.float32, device=s.U[0].device)
+    corr[: s.nc].copy_(s.U[8])
+    return corr
+
+
+def _step_radiation(s, dt, ch, decay, drag_impulse, correction, flags, what):
+    _check_impulse(drag_impulse)
+    if correction.numel() != 9 * s.nc or correction.dtype != torch.float32 or not correction.is_contiguous():
+        raise PMFMHDError(f"{what}: correction must be a contiguous float32 buffer of 9*ncells values")
+    ct = s.ct.packed.data_ptr() if uses_ct(s) else None
+    _check(lib().pmfmhd_step_radiation(context(s.device), ctypes.byref(s.grid), _p9(s.U), _p9(s.scratch), ct,
+                                       correction.data_ptr(), float(dt), float(ch), float(decay),
+                                       float(drag_impulse), int(flags), _stream()), what)
+    s.U, s.scratch = s.scratch, s.U
+    return s
+
+
+def step_ref_radiation(s: MHDState, dt: float, ch: float, decay: float, drag_impulse: float, correction,
+                       track_density: bool = True, track_magnetic: bool = True, track_energy: bool = True,
+                       robust_fallback: bool = False) -> MHDState:
+    """integrator_ref.jl:238-258: the drag step whose face states carry the velocity
+    corrections of ``correction`` (slot 0 = psi), with the tracked density increment and
+    the Kahan remainders of B and E kept in it; CT faces are compensated with
+    ``track_magnetic``. ``robust_fallback`` runs minmod PLM with HLL."""
+    flags = ((RAD_TRACK_DENSITY if track_density else 0) | (RAD_TRACK_MAGNETIC if track_magnetic else 0)
+             | (RAD_TRACK_ENERGY if track_energy else 0) | (RAD_ROBUST_FALLBACK if robust_fallback else 0))
+    return _step_radiation(s, dt, ch, decay, drag_impulse, correction, flags, "step_ref_radiation!")
+
+
+def step_cube_radiation(s: MHDState, dt: float, ch: float, decay: float, drag_impulse: float, correction,
+                        track_density: bool = True, track_magnetic: bool = True, track_energy: bool = True,
+                        check_admissibility: bool = False, fallback: bool = False, global_fallback: bool = False,
+                        robust_fallback: bool = False) -> MHDState:
+    """integrator_cube.jl:504-540 (GLM states): as step_ref_radiation, plus the admissibility
+    flag (rejected cells get density -max(|rho|, max(smallr, llf_dmin))) and the global LLF
+    fallback. The masked per-face fallback (``fallback=True``) is not provided."""
+    if uses_ct(s):
+        raise PMFMHDError("step_cube_radiation!: CT is implemented on the :ref integrator only "
+                          "(mhd_solver=:ct states cannot use the :cube integrators)")
+    if fallback and not global_fallback and not robust_fallback:
+        raise PMFMHDError("step_cube_radiation!: the masked per-face fallback is not provided")
+    flags = ((RAD_TRACK_DENSITY if track_density else 0) | (RAD_TRACK_MAGNETIC if track_magnetic else 0)
+             | (RAD_TRACK_ENERGY if track_energy else 0) | (RAD_CHECK_ADMISSIBILITY if check_admissibility else 0)
+             | (RAD_ROBUST_FALLBACK if robust_fallback else 0) | (RAD_GLOBAL_FALLBACK if global_fallback else 0))
+    return _step_radiation(s, dt, ch, decay, drag_impulse, correction, flags, "step_cube_radiation!")
+
+
 def apply_linear_drag(s: MHDState, decay: float, target_velocity=(0.0, 0.0, 0.0),
                       energy_compensation: Optional[torch.Tensor] = None) -> MHDState:
     """drag.jl:78-117: exact linear drag with velocity decay factor `decay` in [0, 1]."""
@@ -577,6 +634,22 @@ def ct_faces_from_potential(s: MHDState, Ax, Ay, Az) -> MHDState:
                                                 _P3(*[a.data_ptr() for a in A]), _p9(s.U), s.ct.packed.data_ptr(),
                                                 _stream()), "ct_faces_from_potential!")
     torch.cuda.current_stream().synchronize()
+    return s
+
+
+def ct_install_faces(s: MHDState, bxf, byf, bzf) -> MHDState:
+    """ct.jl:228-236 `_ct_install_faces!`: faces set, remainders zeroed, cell B = face
+    average, E keeps the thermal pressure, psi = 0 (on the device)."""
+    if not uses_ct(s):
+        raise PMFMHDError("_ct_install_faces! needs a CT state (mhd_solver=:ct)")
+    dev = s.U[0].device
+    for d, f in enumerate((bxf, byf, bzf)):
+        t = torch.as_tensor(np.asarray(f, dtype=np.float32).ravel()) if not isinstance(f, torch.Tensor) else f
+        if t.numel() != s.nc:
+            raise PMFMHDError(f"face array has {t.numel()} entries, expected {s.nc}")
+        s.ct.slot(d).copy_(t.to(dev, torch.float32).reshape(-1))
+    _check(lib().pmfmhd_ct_install_faces(context(s.device), ctypes.byref(s.grid), _p9(s.U), s.ct.packed.data_ptr(),
+                                         _stream()), "_ct_install_faces!")
     return s
 
 

@@ -190,3 +190,33 @@ def ct_smoke_fields(N, gamma=5 / 3):
     U[0], U[1], U[5], U[6], U[7] = rho, rho * vx, bx, by, bz
     U[4] = T(1) / (g - T(1)) + T(0.5) * rho * vx * vx + T(0.5) * (bx * bx + by * by + bz * bz)
     return U
+
+
+def ct_guide_problem(N, P0=1000.0, amp=2e-4, vamp=1e-4):
+    """Weak oblique perturbation on a strong guide field (test/inherited/test_ct.jl:484-505):
+    the edge potential (3, nc) and the hydro fields (5, nc: rho, momentum, E without magnetic
+    energy), FP32 values of FP64 expressions accumulated in FP32 as the reference does. The
+    faces are the staggered curl of the potential plus the guide field B0 = (35, 22, 28)."""
+    T = np.float32
+    i, j, k = cell_coords((N, N, N))
+    x, y, z = (i - 1) / N, (j - 1) / N, (k - 1) / N
+    modes = ((1, 2, -1, 0.3), (2, -1, 1, 1.1), (-1, 1, 2, 2.0), (3, 1, -2, 0.7), (1, -3, 2, 1.9))
+    nc = N ** 3
+    A = np.zeros((3, nc), T)
+    rho = np.ones(nc, T)
+    v = np.zeros((3, nc), T)
+    amp, vamp = float(T(amp)), float(T(vamp))
+    for m, (a, b, cc, ph) in enumerate(modes, start=1):
+        arg = 2 * np.pi * (a * x + b * y + cc * z) + ph
+        A[0] += (amp * np.sin(arg + m) / (2 * np.pi * (abs(b) + abs(cc)))).astype(T)
+        A[1] += (amp * np.cos(arg) / (2 * np.pi * (abs(a) + abs(cc)))).astype(T)
+        A[2] += (amp * np.sin(arg + 2 * m) / (2 * np.pi * (abs(a) + abs(b)))).astype(T)
+        v[0] += (vamp * np.sin(arg + 0.5 * m)).astype(T)
+        v[1] += (vamp * np.cos(arg + m)).astype(T)
+        v[2] += (vamp * np.sin(arg + 1.5 * m)).astype(T)
+        rho += (1e-3 * np.cos(arg + 2 * m)).astype(T)
+    hyd = np.zeros((5, nc), T)
+    hyd[0] = rho
+    hyd[1:4] = rho * v
+    hyd[4] = T(P0 / (5 / 3 - 1)) + T(0.5) * rho * (v[0] ** 2 + v[1] ** 2 + v[2] ** 2)
+    return A, hyd, (T(35), T(22), T(28))
