@@ -262,6 +262,69 @@ int pmfmhd_set_tile(pmfmhd_ctx* ctx, const pmfmhd_grid* g, int mhd_solver, int c
 int pmfmhd_get_tile(pmfmhd_ctx* ctx, const pmfmhd_grid* g, int mhd_solver, int compensated, int* rows,
                     int* planes);
 
+/* ---- Initial conditions ------------------------------------------------------------- */
+
+/* Mode realizations of the PMF generator (pmf.jl:193-203). The reference's `:legacy`
+ * realization draws from Julia's MersenneTwister and is not provided. */
+#define PMFMHD_PMF_HASH 1            /* :physical_hash */
+#define PMFMHD_PMF_HASH_ZERO_PHASE 2 /* :physical_hash_zero_phase */
+
+/* Arguments of `pmf_batchelor_field` (pmf.jl:300-317); "none" values as noted. */
+typedef struct pmfmhd_pmf_params {
+  int32_t nx, ny, nz;          /* nx even */
+  int32_t realization;         /* PMFMHD_PMF_HASH or PMFMHD_PMF_HASH_ZERO_PHASE */
+  int64_t seed;
+  double box;                  /* box side L */
+  double brms;                 /* target rms (> 0) */
+  double realization_box;      /* <= 0: = box; realization_box / box must be an integer */
+  double kcut;                 /* <= 0: pi * min(dims) / box */
+  double kmin;                 /* >= 0 */
+  double kmax;                 /* <= 0: no band limit */
+  double energy_index;         /* 4: shell energy ~ k^4 */
+  double cutoff_order;         /* 2 */
+  int32_t curl_symbol;         /* 0: centred sin(k dx)/dx, 1: continuum k */
+  int32_t curl_reference_n;    /* 0: none */
+  int32_t fixed_mode_power;    /* rescale every mode to the analytic envelope */
+  int32_t invariant_axis;      /* 0: none, 1..3: modes with k_axis != 0 removed */
+  double preserve_low_kmax;    /* <= 0: none */
+  double preserve_low_kcut;    /* <= 0: = kcut */
+  int32_t normalization;       /* 0: auto, 1: total band rms, 2: reference (low) band rms */
+  int32_t mode_lock_n;         /* 0: none */
+  int32_t high_mode_lock_n;    /* 0: none */
+  int32_t reserved;
+  double minimum_cells_per_wavelength; /* <= 0: not enforced */
+} pmfmhd_pmf_params;
+
+/*
+ * Non-helical Batchelor-spectrum magnetic field (`pmf_batchelor_field`, pmf.jl:300-591) into
+ * three caller arrays of nx*ny*nz floats (x fastest): hashed vector-potential modes keyed
+ * by physical mode number (pmf.jl:109-191), B = i s(k) x A(k) with the kcut taper, the
+ * kmin/kmax band, optional centred-curl reference projection, mode locking, the preserved
+ * low band and fixed mode power, then an inverse real FFT (cuFFT) and the rms
+ * normalisation. stats (nullable): total brms, reference-band brms, normalisation brms,
+ * kcut, kmax, high-source scale. Validation errors are PMFMHD_EINVAL / PMFMHD_ESHAPE, a zero
+ * field PMFMHD_EINADMISSIBLE. Allocates transient workspace (about 5 floats per cell).
+ */
+int pmfmhd_pmf_batchelor_field(pmfmhd_ctx* ctx, const pmfmhd_pmf_params* p, float* const B[3], double stats[6],
+                               void* stream);
+/* dst (nx*ny*nz) = src (sx*sy*sz) repeated periodically; each tile extent must divide the
+ * grid's (`_periodic_tile_field`, pmf.jl:226-237, used by `init_pmf_batchelor_tiled!`). */
+int pmfmhd_periodic_tile(pmfmhd_ctx* ctx, const float* src, int sx, int sy, int sz, float* dst, int nx, int ny,
+                         int nz, void* stream);
+/* Uniform gas around the field in U[5..7] (`_install_pmf_field!`, pmf.jl:239-261):
+ * rho = rho0, zero momentum, E = p0/(gamma-1) + |B|^2/2, psi = 0. */
+int pmfmhd_pmf_install(pmfmhd_ctx* ctx, const pmfmhd_grid* g, float* const U[9], float rho0, float p0,
+                       void* stream);
+/*
+ * Discretely divergence-free CT faces from the cell field U[5..7] (`ct_faces_from_cells!`,
+ * ct.jl:246-308): FP64 cuFFT, projection onto tan(theta).b = 0, half-cell phase shift,
+ * faces installed as by pmfmhd_ct_install_faces. stats (nullable): relative L2 change of the
+ * cell field, magnetic energy ratio, max face div * dx / Brms. Allocates transient FP64
+ * workspace (about 7 doubles per cell).
+ */
+int pmfmhd_ct_faces_from_cells(pmfmhd_ctx* ctx, const pmfmhd_grid* g, float* const U[9], float* ct_packed,
+                               double stats[3], void* stream);
+
 #ifdef __cplusplus
 }
 #endif

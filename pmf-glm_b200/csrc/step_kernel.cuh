@@ -35,6 +35,10 @@ constexpr int PLANE_X0 = 4; // column of x0 in the staged plane
 
 // Threads per CTA: TY+2 row warps and the halo warp.
 template <int TY> __host__ __device__ constexpr int step_threads() { return 32 * (TY + 3); }
+// CTAs per SM the step kernel is compiled for: short tiles fit two per SM (shared memory
+// under half the SM's, registers capped at 128 per thread), so one CTA's barrier waits
+// overlap the other's work.
+template <int TY> __host__ __device__ constexpr int step_min_blocks() { return TY <= 5 ? 2 : 1; }
 
 // Number of CT workspace arrays written by the Godunov stage (reference CTState slots 4-15).
 constexpr int CT_NWORK = 12;
@@ -593,7 +597,7 @@ __device__ __forceinline__ void cta_range(long long Q, long long* q0, long long*
 
 // One box: a persistent launch of one CTA per resident slot.
 template <int TY, int RECON, int RSOL, bool CT, bool COMP, int SRC>
-__global__ void __launch_bounds__(step_threads<TY>(), 1) mhd_step_kernel(const __grid_constant__ StepArgs a) {
+__global__ void __launch_bounds__(step_threads<TY>(), step_min_blocks<TY>()) mhd_step_kernel(const __grid_constant__ StepArgs a) {
   extern __shared__ __align__(128) float smem[];
   __shared__ unsigned long long tma_bar;
   __shared__ int tma_off;
@@ -621,7 +625,7 @@ struct alignas(64) BoxStep {
 };
 
 template <int TY, int RECON, int RSOL, bool CT, bool COMP>
-__global__ void __launch_bounds__(step_threads<TY>(), 1) mhd_batch_kernel(const BoxStep* __restrict__ boxes, int nbox,
+__global__ void __launch_bounds__(step_threads<TY>(), step_min_blocks<TY>()) mhd_batch_kernel(const BoxStep* __restrict__ boxes, int nbox,
                                                                        long long Q) {
   extern __shared__ __align__(128) float smem[];
   __shared__ unsigned long long tma_bar;

@@ -59,6 +59,20 @@ _P3 = ctypes.c_void_p * 3
 _GP = ctypes.POINTER(Grid)
 _F3P = ctypes.POINTER(ctypes.c_float)  # const float[3], nullable
 
+
+class PmfParams(ctypes.Structure):
+    """pmfmhd_pmf_params (include/pmfmhd.h)."""
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+                ("realization", ctypes.c_int32), ("seed", ctypes.c_int64), ("box", ctypes.c_double),
+                ("brms", ctypes.c_double), ("realization_box", ctypes.c_double), ("kcut", ctypes.c_double),
+                ("kmin", ctypes.c_double), ("kmax", ctypes.c_double), ("energy_index", ctypes.c_double),
+                ("cutoff_order", ctypes.c_double), ("curl_symbol", ctypes.c_int32),
+                ("curl_reference_n", ctypes.c_int32), ("fixed_mode_power", ctypes.c_int32),
+                ("invariant_axis", ctypes.c_int32), ("preserve_low_kmax", ctypes.c_double),
+                ("preserve_low_kcut", ctypes.c_double), ("normalization", ctypes.c_int32),
+                ("mode_lock_n", ctypes.c_int32), ("high_mode_lock_n", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("minimum_cells_per_wavelength", ctypes.c_double)]
+
 SIGNATURES = {
     "pmfmhd_version": ([], ctypes.c_int),
     "pmfmhd_strerror": ([ctypes.c_int], ctypes.c_char_p),
@@ -73,6 +87,11 @@ SIGNATURES = {
     "pmfmhd_step_radiation": ([_VP, _GP, _P9, _P9, _VP, _VP, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                ctypes.c_float, ctypes.c_int, _VP], ctypes.c_int),
     "pmfmhd_ct_install_faces": ([_VP, _GP, _P9, _VP, _VP], ctypes.c_int),
+    "pmfmhd_pmf_batchelor_field": ([_VP, ctypes.POINTER(PmfParams), _P3, ctypes.c_double * 6, _VP], ctypes.c_int),
+    "pmfmhd_pmf_install": ([_VP, _GP, _P9, ctypes.c_float, ctypes.c_float, _VP], ctypes.c_int),
+    "pmfmhd_periodic_tile": ([_VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP, ctypes.c_int, ctypes.c_int,
+                              ctypes.c_int, _VP], ctypes.c_int),
+    "pmfmhd_ct_faces_from_cells": ([_VP, _GP, _P9, _VP, ctypes.c_double * 3, _VP], ctypes.c_int),
     "pmfmhd_apply_linear_drag": ([_VP, _GP, _P9, ctypes.c_float, _F3P, _VP, _VP], ctypes.c_int),
     "pmfmhd_apply_exponential_drag_increment": ([_VP, _GP, _P9, _P9, ctypes.c_float, _F3P, _VP], ctypes.c_int),
     "pmfmhd_max_wavespeed": ([_VP, _GP, _P9, ctypes.POINTER(ctypes.c_float), _VP], ctypes.c_int),
@@ -654,56 +673,125 @@ def ct_install_faces(s: MHDState, bxf, byf, bzf) -> MHDState:
 
 
 def ct_faces_from_cells(s: MHDState) -> dict:
-    """ct.jl:246-308: project the cell B onto the CT-admissible subspace (host FP64 FFT),
-    install faces, cell B = face average, E keeps the thermal pressure, psi = 0."""
+    """ct.jl:246-308: project the cell B onto the CT-admissible subspace (FP64 cuFFT on the
+    device), install the faces, cell B = face average, E keeps the thermal pressure, psi = 0."""
     if not uses_ct(s):
         raise PMFMHDError("ct_faces_from_cells! needs a CT state (mhd_solver=:ct)")
+    st = (ctypes.c_double * 3)()
+    _check(lib().pmfmhd_ct_faces_from_cells(context(s.device), ctypes.byref(s.grid), _p9(s.U),
+                                            s.ct.packed.data_ptr(), st, _stream()), "ct_faces_from_cells!")
+    return {"cell_b_rel_l2_change": st[0], "magnetic_energy_ratio": st[1], "max_divb_face_dx_over_brms": st[2]}
+
+
+# ---- primordial magnetic field initial conditions (lib/MHDKernels/src/pmf.jl) ----------------
+
+_REALIZATION = {"physical_hash": 1, "physical_hash_zero_phase": 2}
+
+
+def pmf_batchelor_field(dims, box=1.0, brms=1.0, seed=1, kcut=None, kmin=0.0, kmax=None, energy_index=4.0,
+                        cutoff_order=2.0, mode_lock_n=None, high_mode_lock_n=None, preserve_low_kmax=None,
+                        preserve_low_kcut=None, normalization_kind="auto", curl_symbol="centered",
+                        curl_reference_n=None, fixed_mode_power=False, mode_realization="physical_hash",
+                        realization_box=None, minimum_cells_per_wavelength=None, invariant_axis=0, device=None,
+                        out=None):
+    """pmf.jl:300-591 on the device: returns (Bx, By, Bz, stats), three float32 device arrays of
+    nx*ny*nz values (x fastest). ``out`` may give the three arrays to fill. Only the
+    physical-hash realizations are provided (the reference's ``:legacy`` draws use Julia's
+    MersenneTwister)."""
+    nx, ny, nz = (int(d) for d in dims)
+    mode = str(mode_realization).lower()
+    if mode == "legacy":
+        raise PMFMHDError("mode_realization=:legacy (Julia MersenneTwister draws) is not provided; "
+                          "use :physical_hash or :physical_hash_zero_phase")
+    if mode not in _REALIZATION:
+        raise PMFMHDError("mode_realization must be :legacy, :physical_hash, or :physical_hash_zero_phase")
+    norm = {"auto": 0, "total": 1, "total_band": 1, "total_band_rms": 1, "reference": 2, "reference_band": 2,
+            "low_band": 2, "reference_band_rms": 2}.get(str(normalization_kind).lower())
+    if norm is None:
+        raise PMFMHDError("normalization_kind must be :total_band_rms or :reference_band_rms")
+    curl = {"centered": 0, "continuum": 1, "spectral": 1}.get(str(curl_symbol))
+    if curl is None:
+        raise PMFMHDError("curl_symbol must be :centered or :continuum")
+    p = PmfParams(nx, ny, nz, _REALIZATION[mode], int(seed), float(box), float(brms),
+                  float(realization_box) if realization_box is not None else 0.0,
+                  float(kcut) if kcut is not None else 0.0, float(kmin), float(kmax) if kmax is not None else 0.0,
+                  float(energy_index), float(cutoff_order), curl, int(curl_reference_n or 0), int(bool(fixed_mode_power)),
+                  int(invariant_axis), float(preserve_low_kmax) if preserve_low_kmax is not None else 0.0,
+                  float(preserve_low_kcut) if preserve_low_kcut is not None else 0.0, norm, int(mode_lock_n or 0),
+                  int(high_mode_lock_n or 0), 0,
+                  float(minimum_cells_per_wavelength) if minimum_cells_per_wavelength is not None else 0.0)
+    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    B = out if out is not None else [torch.empty(nx * ny * nz, dtype=torch.float32, device=dev) for _ in range(3)]
+    st = (ctypes.c_double * 6)()
+    _check(lib().pmfmhd_pmf_batchelor_field(context(dev.index), ctypes.byref(p), _P3(*[b.data_ptr() for b in B]), st,
+                                            _stream()), "pmf_batchelor_field")
+    stats = {"brms": float(brms), "brms_measured": st[0], "total_brms_measured": st[0],
+             "reference_band_brms_measured": st[1], "normalization_brms_measured": st[2],
+             "normalization_kind": "reference_band_rms" if (norm == 2 or (norm == 0 and preserve_low_kmax))
+             else "total_band_rms", "box": float(box), "kcut": st[3], "kmax": st[4], "seed": int(seed),
+             "energy_index": float(energy_index), "mode_realization": mode,
+             "realization_box": float(realization_box) if realization_box is not None else float(box),
+             "preserve_high_source_scale": st[5]}
+    return B[0], B[1], B[2], stats
+
+
+def _install_pmf(s: MHDState, rho0, p0):
+    _check(lib().pmfmhd_pmf_install(context(s.device), ctypes.byref(s.grid), _p9(s.U), float(rho0), float(p0),
+                                    _stream()), "_install_pmf_field!")
+    return ct_faces_from_cells(s) if uses_ct(s) else None
+
+
+def init_pmf_batchelor(s: MHDState, brms=None, b0_pG=None, Bunit_pG=1.0, rho0=1.0, p0=1.0, box=None, **kw) -> dict:
+    """pmf.jl:602-642: uniform gas (rho0, p0, at rest, psi = 0) around a Batchelor field
+    generated in place into s.U[5..7]; CT states get faces from ct_faces_from_cells."""
+    if brms is None:
+        if b0_pG is None:
+            raise PMFMHDError("provide either brms code units or b0_pG")
+        brms = float(b0_pG) / float(Bunit_pG)
+    box = s.dims[0] * s.dx if box is None else box
+    *_, stats = pmf_batchelor_field(s.dims, box=box, brms=brms, device=s.device, out=[s.U[5], s.U[6], s.U[7]], **kw)
+    ctinfo = _install_pmf(s, rho0, p0)
+    stats.update(rho0=float(rho0), p0=float(p0), Bunit_pG=float(Bunit_pG))
+    if ctinfo is not None:
+        stats["ct_faces"] = ctinfo
+    return stats
+
+
+def init_pmf_batchelor_tiled(s: MHDState, tile_box, tile_n=None, brms=None, b0_pG=None, Bunit_pG=1.0, rho0=1.0,
+                             p0=1.0, box=None, **kw) -> dict:
+    """pmf.jl:652-700: a field generated on a smaller periodic tile of side tile_box (tile_n
+    cells) and repeated through the box."""
+    if brms is None:
+        if b0_pG is None:
+            raise PMFMHDError("provide either brms code units or b0_pG")
+        brms = float(b0_pG) / float(Bunit_pG)
+    L = float(s.dims[0] * s.dx if box is None else box)
+    Lt = float(tile_box)
+    if not Lt > 0:
+        raise PMFMHDError("tile_box must be positive")
+    if not Lt <= L:
+        raise PMFMHDError("tile_box cannot exceed full box")
+    n = s.dims[0]
+    nt = int(round(n * Lt / L)) if tile_n is None else int(tile_n)
+    if nt <= 0:
+        raise PMFMHDError("tile_n must be positive")
+    if nt > n:
+        raise PMFMHDError("tile_n cannot exceed target grid size")
+    if n % nt:
+        raise PMFMHDError(f"tile_n={nt} must divide target grid size {n}")
+    if not abs(Lt / L - nt / n) <= 4 * np.finfo(float).eps * max(1, Lt / L):
+        raise PMFMHDError("tile_box/full box must match tile_n/target_n")
+    Bt = pmf_batchelor_field((nt, nt, nt), box=Lt, brms=brms, device=s.device, **kw)
     nx, ny, nz = s.dims
-    h = fields_to_host(s).astype(np.float64)
-    Bold = [h[5 + d].reshape(nz, ny, nx) for d in range(3)]
-    Bh = [np.fft.rfftn(b) for b in Bold]  # axes (z, y, x); rfft along x
-
-    def half_phase(n, m):
-        mm = np.where(m > n / 2, m - n, m)
-        nyq = (n % 2 == 0) & (m == n // 2)
-        return np.where(nyq, 0.0, np.pi * mm / n), nyq
-
-    tx, nqx = half_phase(nx, np.arange(nx // 2 + 1))
-    ty, nqy = half_phase(ny, np.arange(ny))
-    tz, nqz = half_phase(nz, np.arange(nz))
-    thz, thy, thx = np.meshgrid(tz, ty, tx, indexing="ij")
-    nyz, nyy, nyx = np.meshgrid(nqz, nqy, nqx, indexing="ij")
-    bx = np.where(nyx, 0, Bh[0]); by = np.where(nyy, 0, Bh[1]); bz = np.where(nyz, 0, Bh[2])
-    tnx, tny, tnz = np.tan(thx), np.tan(thy), np.tan(thz)
-    t2 = tnx * tnx + tny * tny + tnz * tnz
-    dot = np.where(t2 > 0, (tnx * bx + tny * by + tnz * bz) / np.where(t2 > 0, t2, 1.0), 0)
-    bx = bx - tnx * dot; by = by - tny * dot; bz = bz - tnz * dot
-    Fx = bx * np.exp(-1j * thx) / np.cos(thx)
-    Fy = by * np.exp(-1j * thy) / np.cos(thy)
-    Fz = bz * np.exp(-1j * thz) / np.cos(thz)
-    faces = [np.fft.irfftn(F, s=(nz, ny, nx), axes=(0, 1, 2)).ravel() for F in (Fx, Fy, Fz)]
-    dev = torch.device("cuda", s.device)
-    s.ct.slot(18).zero_(); s.ct.slot(19).zero_(); s.ct.slot(20).zero_()
     for d in range(3):
-        s.ct.slot(d).copy_(torch.from_numpy(faces[d].astype(np.float32)).to(dev))
-    # cell B <- face average, E keeps p, psi <- 0 (ct.jl:205-219), done on the host in FP32
-    f32 = [f.astype(np.float32).reshape(nz, ny, nx) for f in faces]
-    hb = fields_to_host(s)
-    bxc = (np.float32(0.5) * (f32[0] + np.roll(f32[0], -1, axis=2))).ravel()
-    byc = (np.float32(0.5) * (f32[1] + np.roll(f32[1], -1, axis=1))).ravel()
-    bzc = (np.float32(0.5) * (f32[2] + np.roll(f32[2], -1, axis=0))).ravel()
-    ox, oy, oz = hb[5], hb[6], hb[7]
-    hb[4] = hb[4] + np.float32(0.5) * ((bxc * bxc + byc * byc + bzc * bzc) - (ox * ox + oy * oy + oz * oz))
-    hb[5], hb[6], hb[7], hb[8] = bxc, byc, bzc, 0
-    set_fields(s, hb)
-    Bnew = [hb[5 + d].astype(np.float64) for d in range(3)]
-    num = sum(((Bnew[d] - Bold[d].ravel()) ** 2).sum() for d in range(3))
-    den = sum((Bold[d] ** 2).sum() for d in range(3))
-    enew = sum((Bnew[d] ** 2).sum() for d in range(3))
-    brms = np.sqrt(enew / s.nc)
-    return {"cell_b_rel_l2_change": float(np.sqrt(num / den)) if den > 0 else 0.0,
-            "magnetic_energy_ratio": float(enew / den) if den > 0 else 1.0,
-            "max_divb_face_dx_over_brms": float(max_divb_face(s) * s.dx / brms) if brms > 0 else 0.0}
+        _check(lib().pmfmhd_periodic_tile(context(s.device), Bt[d].data_ptr(), nt, nt, nt, s.U[5 + d].data_ptr(),
+                                          nx, ny, nz, _stream()), "_periodic_tile_field")
+    stats = dict(Bt[3])
+    ctinfo = _install_pmf(s, rho0, p0)
+    stats.update(rho0=float(rho0), p0=float(p0), Bunit_pG=float(Bunit_pG), full_box=L, tile_box=Lt, tile_n=nt)
+    if ctinfo is not None:
+        stats["ct_faces"] = ctinfo
+    return stats
 
 
 # ---- batched boxes ---------------------------------------------------------------------
