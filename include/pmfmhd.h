@@ -262,6 +262,37 @@ int pmfmhd_set_tile(pmfmhd_ctx* ctx, const pmfmhd_grid* g, int mhd_solver, int c
 int pmfmhd_get_tile(pmfmhd_ctx* ctx, const pmfmhd_grid* g, int mhd_solver, int compensated, int* rows,
                     int* planes);
 
+/* ---- Terminal-regime induction (terminal_ct.jl) -------------------------------------- */
+/* All on cubic periodic grids (PMFMHD_ESHAPE / PMFMHD_EUNSUPPORTED otherwise). */
+
+/* Centred conservative Maxwell-stress force of B into F (`terminal_magnetic_force!`,
+ * terminal_ct.jl:18-51,99-106). With P non-null the force is split (`..._split!`, :53-69,
+ * :117-126): P = magnetic pressure -grad(B^2/2), F = the tension remainder. */
+int pmfmhd_terminal_magnetic_force(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const B[3],
+                                   float* const F[3], float* const P[3], void* stream);
+/* Max terminal speed |v|, v = (F - c_p grad rho)/(max(rho, smallr) Gamma) capped at vcap
+ * (`terminal_velocity_max!`, terminal_ct.jl:125-145,226-238). Reads U[0], U[5..7]. Blocking. */
+int pmfmhd_terminal_velocity_max(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], float gamma_drag,
+                                 float pressure_coeff, float vcap, double* vmax, void* stream);
+/*
+ * Terminal-regime SSPRK2 induction over dt (`terminal_ct_induction!`, terminal_ct.jl:502-575):
+ * nsub = ceil(dt vmax / (cfl dx)) subcycles (PMFMHD_EINADMISSIBLE above max_subcycles), EMF
+ * v x B from the terminal velocity recomputed at both stages, centred curl (GLM, ct_packed
+ * NULL) or edge-averaged face curl (CT, faces Kahan-compensated through the packed
+ * remainders when `compensate`), order-2 or order-4 dissipation with eta from vmax; E
+ * follows the magnetic energy. Density and thermal energy are held. scratch (9 arrays) and
+ * the CT workspace slots are overwritten. Outputs nsub, vmax, eta (nullable).
+ */
+int pmfmhd_terminal_ct_induction(pmfmhd_ctx* ctx, const pmfmhd_grid* g, float* const U[9], float* const scratch[9],
+                                 float* ct_packed, float dt, float gamma_drag, float pressure_coeff, float cfl,
+                                 float dissipation, int dissipation_order, float vcap, int max_subcycles,
+                                 int compensate, int* nsub, double* vmax, double* eta, void* stream);
+/* One compensated forward-Euler face update from the cell EMFs the caller left in the CT
+ * slots ecx/ecy/ecz, then cell B = face average with E following and psi = 0
+ * (`terminal_ct_euler_from_cell_emf!`, terminal_ct.jl:461-486). */
+int pmfmhd_terminal_ct_euler_from_cell_emf(pmfmhd_ctx* ctx, const pmfmhd_grid* g, float* const U[9],
+                                           float* ct_packed, float dt, void* stream);
+
 /* ---- Initial conditions ------------------------------------------------------------- */
 
 /* Mode realizations of the PMF generator (pmf.jl:193-203). The reference's `:legacy`

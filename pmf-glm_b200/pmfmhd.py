@@ -87,6 +87,14 @@ SIGNATURES = {
     "pmfmhd_step_radiation": ([_VP, _GP, _P9, _P9, _VP, _VP, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                ctypes.c_float, ctypes.c_int, _VP], ctypes.c_int),
     "pmfmhd_ct_install_faces": ([_VP, _GP, _P9, _VP, _VP], ctypes.c_int),
+    "pmfmhd_terminal_magnetic_force": ([_VP, _GP, _P3, _P3, _VP, _VP], ctypes.c_int),
+    "pmfmhd_terminal_velocity_max": ([_VP, _GP, _P9, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                      ctypes.POINTER(ctypes.c_double), _VP], ctypes.c_int),
+    "pmfmhd_terminal_ct_induction": ([_VP, _GP, _P9, _P9, _VP, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                      ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_float, ctypes.c_int,
+                                      ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_double), _VP], ctypes.c_int),
+    "pmfmhd_terminal_ct_euler_from_cell_emf": ([_VP, _GP, _P9, _VP, ctypes.c_float, _VP], ctypes.c_int),
     "pmfmhd_pmf_batchelor_field": ([_VP, ctypes.POINTER(PmfParams), _P3, ctypes.c_double * 6, _VP], ctypes.c_int),
     "pmfmhd_pmf_install": ([_VP, _GP, _P9, ctypes.c_float, ctypes.c_float, _VP], ctypes.c_int),
     "pmfmhd_periodic_tile": ([_VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP, ctypes.c_int, ctypes.c_int,
@@ -681,6 +689,77 @@ def ct_faces_from_cells(s: MHDState) -> dict:
     _check(lib().pmfmhd_ct_faces_from_cells(context(s.device), ctypes.byref(s.grid), _p9(s.U),
                                             s.ct.packed.data_ptr(), st, _stream()), "ct_faces_from_cells!")
     return {"cell_b_rel_l2_change": st[0], "magnetic_energy_ratio": st[1], "max_divb_face_dx_over_brms": st[2]}
+
+
+# ---- terminal-regime induction (lib/MHDKernels/src/terminal_ct.jl) ---------------------------
+
+def _cubic(s, what):
+    if not all(d == s.dims[0] for d in s.dims):
+        raise PMFMHDError(f"{what} requires a cubic grid")
+
+
+def terminal_magnetic_force(s: MHDState, fx, fy, fz, B=None):
+    """terminal_ct.jl:99-106: centred conservative Maxwell-stress force of B (default s.U[5..7])."""
+    _cubic(s, "terminal magnetic force")
+    B = B if B is not None else (s.U[5], s.U[6], s.U[7])
+    _check(lib().pmfmhd_terminal_magnetic_force(context(s.device), ctypes.byref(s.grid), _P3(*[b.data_ptr() for b in B]),
+                                                _P3(fx.data_ptr(), fy.data_ptr(), fz.data_ptr()), None, _stream()),
+           "terminal_magnetic_force!")
+    return fx, fy, fz
+
+
+def terminal_magnetic_force_split(s: MHDState, px, py, pz, tx, ty, tz, B=None):
+    """terminal_ct.jl:117-126: magnetic pressure -grad(B^2/2) and the tension remainder."""
+    _cubic(s, "terminal magnetic force")
+    B = B if B is not None else (s.U[5], s.U[6], s.U[7])
+    _check(lib().pmfmhd_terminal_magnetic_force(context(s.device), ctypes.byref(s.grid), _P3(*[b.data_ptr() for b in B]),
+                                                _P3(tx.data_ptr(), ty.data_ptr(), tz.data_ptr()),
+                                                _P3(px.data_ptr(), py.data_ptr(), pz.data_ptr()), _stream()),
+           "terminal_magnetic_force_split!")
+    return px, py, pz, tx, ty, tz
+
+
+def terminal_velocity_max(s: MHDState, gamma_drag: float, pressure_coeff: float, vcap: float = float("inf")) -> float:
+    """terminal_ct.jl:226-238."""
+    _cubic(s, "terminal CT")
+    out = ctypes.c_double()
+    _check(lib().pmfmhd_terminal_velocity_max(context(s.device), ctypes.byref(s.grid), _p9(s.U), float(gamma_drag),
+                                              float(pressure_coeff), float(vcap), ctypes.byref(out), _stream()),
+           "terminal_velocity_max!")
+    return out.value
+
+
+def terminal_ct_induction(s: MHDState, dt: float, gamma_drag: float, pressure_coeff: float, cfl: float = 0.4,
+                          dissipation: float = 0.05, dissipation_order: int = 4, vcap: float = float("inf"),
+                          max_subcycles: int = 256, compensate: bool = True):
+    """terminal_ct.jl:502-575: returns (nsubcycles, vmax, eta)."""
+    _cubic(s, "terminal CT")
+    if not 0 < cfl <= 1:
+        raise PMFMHDError("terminal CT cfl must be in (0,1]")
+    if not 0 <= dissipation <= 1:
+        raise PMFMHDError("terminal CT dissipation must be in [0,1]")
+    if dissipation_order not in (2, 4):
+        raise PMFMHDError("terminal CT dissipation_order must be 2 or 4")
+    nsub, vmax, eta = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
+    ct = s.ct.packed.data_ptr() if uses_ct(s) else None
+    rc = lib().pmfmhd_terminal_ct_induction(context(s.device), ctypes.byref(s.grid), _p9(s.U), _p9(s.scratch), ct,
+                                            float(dt), float(gamma_drag), float(pressure_coeff), float(cfl),
+                                            float(dissipation), int(dissipation_order), float(vcap), int(max_subcycles),
+                                            int(bool(compensate)), ctypes.byref(nsub), ctypes.byref(vmax),
+                                            ctypes.byref(eta), _stream())
+    if rc == -5:
+        raise PMFMHDError(f"terminal CT needs more than {max_subcycles} subcycles (limit {max_subcycles})")
+    _check(rc, "terminal_ct_induction!")
+    return nsub.value, vmax.value, eta.value
+
+
+def terminal_ct_euler_from_cell_emf(s: MHDState, dt: float) -> None:
+    """terminal_ct.jl:476-486: faces += dt curl(edge average of ct.ec*), compensated."""
+    if not uses_ct(s):
+        raise PMFMHDError("terminal_ct_euler_from_cell_emf! needs a CT state")
+    _check(lib().pmfmhd_terminal_ct_euler_from_cell_emf(context(s.device), ctypes.byref(s.grid), _p9(s.U),
+                                                        s.ct.packed.data_ptr(), float(dt), _stream()),
+           "terminal_ct_euler_from_cell_emf!")
 
 
 # ---- primordial magnetic field initial conditions (lib/MHDKernels/src/pmf.jl) ----------------

@@ -220,3 +220,30 @@ def ct_guide_problem(N, P0=1000.0, amp=2e-4, vamp=1e-4):
     hyd[1:4] = rho * v
     hyd[4] = T(P0 / (5 / 3 - 1)) + T(0.5) * rho * (v[0] ** 2 + v[1] ** 2 + v[2] ** 2)
     return A, hyd, (T(35), T(22), T(28))
+
+
+def terminal_seed(N, amp=0.08):
+    """Terminal-regime seed state (test/inherited/test_terminal_ct.jl:133-155), FP32:
+    rho = 1 + 0.02 sin(x+y), B = amp (sin y, sin z, sin x), thermal energy 1.5, gas at rest.
+    Returns rho, E, (Bx, By, Bz) as flat arrays."""
+    T = np.float32
+    i, j, k = cell_coords((N, N, N))
+    x = (2 * np.pi * (i - 1) / N).astype(T)
+    y = (2 * np.pi * (j - 1) / N).astype(T)
+    z = (2 * np.pi * (k - 1) / N).astype(T)
+    rho = T(1) + T(0.02) * np.sin(x + y)
+    B = [T(amp) * np.sin(y), T(amp) * np.sin(z), T(amp) * np.sin(x)]
+    E = T(1.5) + T(0.5) * (B[0] ** 2 + B[1] ** 2 + B[2] ** 2)
+    return rho.astype(T), E.astype(T), [b.astype(T) for b in B]
+
+
+def terminal_abc(N, amp=0.08, dtype=np.float64):
+    """ABC-type field of the CT/GLM terminal equivalence test
+    (test/inherited/test_terminal_ct_equivalence.jl:40-62): each component independent of its
+    own coordinate, so cell and face values coincide. Returns rho, (Bx, By, Bz) in `dtype`."""
+    i, j, k = cell_coords((N, N, N))
+    x, y, z = 2 * np.pi * (i - 1) / N, 2 * np.pi * (j - 1) / N, 2 * np.pi * (k - 1) / N
+    rho = 1 + 0.02 * np.sin(x + y)
+    B = [amp * (np.sin(y + 0.3) + 0.5 * np.cos(z)), amp * (np.sin(z + 0.7) + 0.5 * np.cos(x)),
+         amp * (np.sin(x + 1.1) + 0.5 * np.cos(y))]
+    return rho.astype(dtype), [b.astype(dtype) for b in B]
