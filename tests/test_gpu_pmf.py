@@ -157,3 +157,24 @@ def test_pmf_argument_errors():
     s = pmfmhd.allocate_state((32, 32, 32), 1.0 / 32)
     with pytest.raises(pmfmhd.PMFMHDError):
         pmfmhd.init_pmf_batchelor_tiled(s, tile_box=0.3, brms=1.0)
+
+
+def test_checkpoint_round_trip_of_a_device_state(tmp_path):
+    """runner.jl:26-140 semantics on device arrays: a CT state written and restored into a
+    fresh state steps to the same bits."""
+    import checkpoint
+    n = 16
+    a = pmfmhd.allocate_state((n, n, n), 1.0 / n, mhd_solver="ct")
+    pmfmhd.init_pmf_batchelor(a, brms=0.3, seed=5, kcut=6 * PI)
+    cfg = {"N": n, "mhd_solver": "ct", "cfl": 0.3}
+    path = str(tmp_path / "ck.bin")
+    checkpoint.write_pmf_checkpoint(path, cfg, {"cycle": 11}, checkpoint.state_arrays(a))
+    b = pmfmhd.allocate_state((n, n, n), 1.0 / n, mhd_solver="ct")
+    rt = checkpoint.restore_pmf_checkpoint(path, cfg, checkpoint.state_arrays(b))
+    assert rt["cycle"] == 11
+    for _ in range(3):
+        dt, _ = pmfmhd.compute_dt(a, 0.3)
+        pmfmhd.step(a, float(dt), integrator="ref")
+        pmfmhd.step(b, float(dt), integrator="ref")
+    assert np.array_equal(pmfmhd.fields_to_host(a), pmfmhd.fields_to_host(b))
+    assert torch.equal(a.ct.packed[: 3 * n ** 3], b.ct.packed[: 3 * n ** 3])
