@@ -82,6 +82,20 @@ int pmfmhd_step_glm(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[
                     float dt, float ch, float decay, float* const resid[7], void* stream);
 
 /*
+ * The GLM step of pmfmhd_step_glm on HOST buffers: Uh (9 host arrays) in, Unh (9 host arrays)
+ * out, for a caller whose state lives in host memory (the reference's CPU-resident
+ * `MHDState`, whose `step_ref!` this replaces for that case). The box is cut into `nchunks`
+ * z-slabs (<= 0: 8; each at least 2 planes): slabs are copied in on one stream, stepped on a
+ * second once their neighbours have arrived, and copied out on a third, so the PCIe traffic
+ * both ways overlaps the compute. Pinned host memory (cudaHostAlloc / cudaHostRegister) is
+ * needed for the overlap; pageable memory works, serialised. Ordered after the caller's
+ * stream; returns after Unh is complete. Device copies of the state are context workspace
+ * (18 floats per cell, kept for the next call). No compensation (resid is not supported).
+ */
+int pmfmhd_step_glm_host(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const Uh[9], float* const Unh[9],
+                         float dt, float ch, float decay, int nchunks, void* stream);
+
+/*
  * One constrained-transport step (mhd_solver=:ct): Godunov stage with the staggered
  * normal field on every face, Gardiner-Stone 2005 edge EMFs, face curl update and the
  * face-averaged cell B. Replaces `step!`'s CT branch: `step_ref!(s, dt; ch=0, decay=1)`

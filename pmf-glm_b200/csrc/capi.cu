@@ -169,7 +169,11 @@ int launch_step(pmfmhd_ctx* c, const pmfmhd_grid* g, StepArgs& a, Tune t, bool c
   a.P = phys_of(g);
   a.status = c->d_status;
   a.use_tma = field_maps(c, g, a.U, t.ty, a.tmap) ? 1 : 0;
-  const long long Q = (long long)a.ntx * a.nty * g->nz;
+  if (a.zhi <= a.zlo) {  // the whole box unless the caller set a plane range
+    a.zlo = 0;
+    a.zhi = g->nz;
+  }
+  const long long Q = (long long)a.ntx * a.nty * (a.zhi - a.zlo);
   const long long slots = (long long)c->sms * occ;
   const long long by_work = std::max<long long>(1, (Q + t.tz - 1) / std::max(1, t.tz));
   const long long blocks = std::min(slots, by_work);
@@ -330,6 +334,11 @@ int pmfmhd_destroy(pmfmhd_ctx* c) {
   cudaFree(c->d_tot);
   cudaFree(c->d_status);
   cudaFreeHost(c->h_pin);
+  cudaFree(c->hp.dev);
+  for (auto& e : c->hp.ev) cudaEventDestroy(e);
+  if (c->hp.start) cudaEventDestroy(c->hp.start);
+  for (auto& st : c->hp.s)
+    if (st) cudaStreamDestroy(st);
   delete c;
   return PMFMHD_OK;
 }
@@ -357,6 +366,81 @@ int pmfmhd_step_ct(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9],
   bool comp;
   if ((rc = resid_mode(resid, &comp))) return rc;
   return enqueue_ct(c, g, U, Unew, ct_packed, dt, resid, comp, compensate_faces != 0, as_stream(stream), nullptr);
+}
+
+int pmfmhd_step_glm_host(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const Uh[9], float* const Unh[9],
+                         float dt, float ch, float decay, int nchunks, void* stream) {
+  if (c == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!nonnull(Uh, 9) || !nonnull(Unh, 9)) return PMFMHD_EINVAL;
+  if (!std::isfinite(dt) || !std::isfinite(ch) || !std::isfinite(decay) || !(ch > 0.0f)) return PMFMHD_EINVAL;
+  const int nz = g->nz;
+  int C = nchunks > 0 ? nchunks : 8;
+  C = std::max(1, std::min(C, nz / 2));  // every chunk at least 2 planes: halos reach chunks c +- 1
+  const long long nc = ncells(g), nxy = (long long)g->nx * g->ny;
+  HostPath& hp = c->hp;
+  const size_t need = 18 * (size_t)nc;
+  if (hp.floats < need) {
+    cudaFree(hp.dev);
+    hp.dev = nullptr;
+    hp.floats = 0;
+    PMF_CK(cudaMalloc(&hp.dev, need * sizeof(float)));
+    hp.floats = need;
+  }
+  for (auto& st : hp.s)
+    if (!st) PMF_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  if (!hp.start) PMF_CK(cudaEventCreateWithFlags(&hp.start, cudaEventDisableTiming));
+  while (hp.ev.size() < 3 * (size_t)C) {
+    cudaEvent_t e;
+    PMF_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    hp.ev.push_back(e);
+  }
+  cudaStream_t caller = as_stream(stream), sin = hp.s[0], scomp = hp.s[1], sout = hp.s[2];
+  const float* Ud[9];
+  float* Und[9];
+  for (int f = 0; f < 9; ++f) {
+    Ud[f] = hp.dev + (size_t)f * nc;
+    Und[f] = hp.dev + (size_t)(9 + f) * nc;
+  }
+  auto zb = [&](int k) { return (int)((long long)nz * k / C); };  // chunk k = planes [zb(k), zb(k+1))
+  auto arrived = [&](int k) { return hp.ev[3 * k]; };
+  auto computed = [&](int k) { return hp.ev[3 * k + 1]; };
+  // ordered after the caller's prior work
+  PMF_CK(cudaEventRecord(hp.start, caller));
+  PMF_CK(cudaStreamWaitEvent(sin, hp.start, 0));
+  PMF_CK(cudaStreamWaitEvent(scomp, hp.start, 0));
+  PMF_CK(cudaStreamWaitEvent(sout, hp.start, 0));
+  // copy in: the last chunk first (the periodic lower halo of chunk 0), then 0, 1, ...
+  for (int i = 0; i < C; ++i) {
+    const int k = (i == 0) ? C - 1 : i - 1;
+    const size_t off = (size_t)zb(k) * nxy, len = (size_t)(zb(k + 1) - zb(k)) * nxy;
+    for (int f = 0; f < 9; ++f)
+      PMF_CK(cudaMemcpyAsync(const_cast<float*>(Ud[f]) + off, Uh[f] + off, len * sizeof(float),
+                             cudaMemcpyHostToDevice, sin));
+    PMF_CK(cudaEventRecord(arrived(k), sin));
+  }
+  // compute chunk k once chunks k-1, k, k+1 (periodic) are resident; copy it out as soon as done
+  const float dtdx = dt / g->dx;
+  const Tune t = tune_for(c, g, false, false);
+  PMF_CK(cudaMemsetAsync(c->d_smax, 0, sizeof(unsigned int), scomp));
+  for (int k = 0; k < C; ++k) {
+    for (int d = -1; d <= 1; ++d) PMF_CK(cudaStreamWaitEvent(scomp, arrived(((k + d) % C + C) % C), 0));
+    StepArgs a;
+    fill_glm_args(a, Ud, Und, nullptr, false, dtdx, ch, decay, c->d_smax);
+    a.zlo = zb(k);
+    a.zhi = zb(k + 1);
+    if ((rc = launch_step(c, g, a, t, false, false, scomp))) return rc;
+    PMF_CK(cudaEventRecord(computed(k), scomp));
+    PMF_CK(cudaStreamWaitEvent(sout, computed(k), 0));
+    const size_t off = (size_t)zb(k) * nxy, len = (size_t)(zb(k + 1) - zb(k)) * nxy;
+    for (int f = 0; f < 9; ++f)
+      PMF_CK(cudaMemcpyAsync(Unh[f] + off, Und[f] + off, len * sizeof(float), cudaMemcpyDeviceToHost, sout));
+  }
+  PMF_CK(cudaEventRecord(hp.ev[3 * (C - 1) + 2], sout));
+  PMF_CK(cudaStreamWaitEvent(caller, hp.ev[3 * (C - 1) + 2], 0));
+  PMF_CK(cudaStreamSynchronize(sout));  // the host buffers are complete on return
+  return PMFMHD_OK;
 }
 
 int pmfmhd_step_glm_drag(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],

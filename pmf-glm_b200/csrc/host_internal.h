@@ -61,6 +61,20 @@ int occupancy_of(const StepKernelInfo& k);
 }  // namespace host
 }  // namespace pmf
 
+namespace pmf {
+namespace host {
+// Workspace of the host-buffer step (pmfmhd_step_glm_host): device copies of the state in and
+// out, three streams (copy in, compute, copy out) and per-chunk events, created on first use.
+struct HostPath {
+  float* dev = nullptr;     // 18 * cells floats: U then Unew
+  size_t floats = 0;
+  cudaStream_t s[3] = {nullptr, nullptr, nullptr};
+  std::vector<cudaEvent_t> ev;  // 3 per chunk: arrived, computed, copied out
+  cudaEvent_t start = nullptr;
+};
+}  // namespace host
+}  // namespace pmf
+
 struct pmfmhd_ctx {
   int device = 0;
   int sms = 148;
@@ -74,6 +88,7 @@ struct pmfmhd_ctx {
   std::vector<pmf::host::GraphEntry> graphs;
   std::map<pmf::host::MapKey, CUtensorMap> maps;  // TMA descriptors of field arrays
   unsigned int* d_status = nullptr;                // device status bits of the step kernels
+  pmf::host::HostPath hp;                          // host-buffer step workspace
   std::mutex mu;
 };
 

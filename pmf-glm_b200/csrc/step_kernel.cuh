@@ -60,6 +60,7 @@ struct StepArgs {
   int use_tma;              // the tensor maps below describe U (fields with nx % 4 == 0)
   CUtensorMap tmap[9];      // per field: 3-D (x, y, z) FP32 map, box (PLANE_W, TY+4, 1)
   DragCoef drag;            // source-coupled steps: drag coefficients (read by SRC_DRAG/SRC_RAD kernels)
+  int zlo, zhi;             // single-box launches: the planes [zlo, zhi) this launch updates
   float* corr;              // SRC_RAD: packed 9*nc correction buffer (slot 0 psi, 1-3 velocity
                             // corrections, 4 density increments, 5-7 B / 8 E remainders)
   int rad_flags;            // SRC_RAD: RAD_* bits
@@ -604,12 +605,14 @@ __global__ void __launch_bounds__(step_threads<TY>(), step_min_blocks<TY>()) mhd
   unsigned tma_phase = 0;
   init_tma_barrier(&tma_bar, &tma_off);
   long long q, qe;
-  cta_range((long long)a.ntx * a.nty * a.nz, &q, &qe);
+  const int nzr = a.zhi - a.zlo;  // planes of this launch
+  cta_range((long long)a.ntx * a.nty * nzr, &q, &qe);
   float smax = 0.0f;
   while (q < qe) {
-    const int col = (int)(q / a.nz);
-    const int z0 = (int)(q - (long long)col * a.nz);
-    const int z1 = (int)min((long long)a.nz, z0 + (qe - q));
+    const int col = (int)(q / nzr);
+    const int zr = (int)(q - (long long)col * nzr);
+    const int z0 = a.zlo + zr;
+    const int z1 = a.zlo + (int)min((long long)nzr, zr + (qe - q));
     march_column<TY, RECON, RSOL, CT, COMP, SRC>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar,
                                                   tma_phase, &tma_off);
     q += z1 - z0;

@@ -80,6 +80,8 @@ SIGNATURES = {
     "pmfmhd_create": ([ctypes.c_int, ctypes.POINTER(_VP)], ctypes.c_int),
     "pmfmhd_destroy": ([_VP], ctypes.c_int),
     "pmfmhd_step_glm": ([_VP, _GP, _P9, _P9, ctypes.c_float, ctypes.c_float, ctypes.c_float, _VP, _VP], ctypes.c_int),
+    "pmfmhd_step_glm_host": ([_VP, _GP, _P9, _P9, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, _VP],
+                             ctypes.c_int),
     "pmfmhd_step_ct": ([_VP, _GP, _P9, _P9, _VP, ctypes.c_float, _VP, ctypes.c_int, _VP], ctypes.c_int),
     "pmfmhd_step_glm_drag": ([_VP, _GP, _P9, _P9, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                               _F3P, _VP], ctypes.c_int),
@@ -294,6 +296,17 @@ def step_cube(s: MHDState, dt: float, ch: float, decay: float) -> MHDState:
                                  float(ch), float(decay), _resid_arg(s), _stream()), "step_cube!")
     s.U, s.scratch = s.scratch, s.U
     return s
+
+
+def step_cube_host(s: MHDState, U_host: torch.Tensor, Unew_host: torch.Tensor, dt: float, ch: float, decay: float,
+                   nchunks: int = 8) -> None:
+    """The GLM step on host (9, nc) float32 tensors (pinned for PCIe/compute overlap) with the
+    grid and parameters of ``s`` (pmfmhd_step_glm_host); ``s``'s device fields are not used."""
+    for t in (U_host, Unew_host):
+        if t.device.type != "cpu" or t.dtype != torch.float32 or tuple(t.shape) != (9, s.nc) or not t.is_contiguous():
+            raise PMFMHDError("host state must be a contiguous float32 CPU tensor of shape (9, ncells)")
+    _check(lib().pmfmhd_step_glm_host(context(s.device), ctypes.byref(s.grid), _p9(U_host), _p9(Unew_host), float(dt),
+                                      float(ch), float(decay), int(nchunks), _stream()), "step_cube_host")
 
 
 def step_ref(s: MHDState, dt: float, ch: float, decay: float, compensate_faces: bool = False) -> MHDState:
