@@ -182,6 +182,59 @@ def linf_vs_fp64(n=64, steps=20):
     return out
 
 
+def build_boxes(specs):
+    """Device states of the batched workload's boxes (host ICs from the seeded generator)."""
+    import ics
+    import pmfmhd
+    states = []
+    for sp in specs:
+        n = sp["n"]
+        b = ics.turbulent_box(n, seed=sp["seed"], beta=sp["beta"], b_index=sp["b_index"], kc=sp["kc"],
+                              with_ct=sp["ct"])
+        s = pmfmhd.set_fields(pmfmhd.allocate_state((n, n, n), 1.0 / n, mhd_solver="ct" if sp["ct"] else "glm"),
+                              b["U"])
+        if sp["ct"]:
+            pmfmhd.ct_faces_from_potential(s, *b["A_edge"])
+        states.append(s)
+    return states
+
+
+def sharded_batched_mix(rank, world, steps=30, nbox=64):
+    """The batched workload on `world` GPUs: boxes placed by LPT on N^3 x steps (sharding.py),
+    one batch per rank, no collective in the step; value = all zone-updates / max-over-ranks
+    device time. Every rank takes the same collective calls."""
+    import torch
+    import torch.distributed as dist
+
+    import ics
+    import pmfmhd
+    import sharding
+    specs = ics.batch_mix(nbox)
+    costs = [sp["n"] ** 3 * steps for sp in specs]
+    mine = [specs[i] for i in sharding.lpt_shard(costs, world)[rank]]
+    states = build_boxes(mine)
+    ms, finite = 0.0, True
+    b = pmfmhd.Batch(states, cfl=0.2) if states else None
+    if b is not None:
+        b.step(2)  # records the graphs
+    dist.barrier()
+    torch.cuda.synchronize()
+    if b is not None:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b.step(steps)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        finite = all(np.isfinite(b.current_fields(i)).all() for i in range(len(states)))
+        b.close()
+    t = torch.tensor([ms, 0.0 if finite else 1.0], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return {"value": sum(costs) / (float(t[0]) / 1e3), "unit": "zone-updates/s", "ranks": world,
+            "boxes": nbox, "steps": steps, "placement": "LPT on N^3 x steps", "max_rank_ms": float(t[0]),
+            "finite": bool(t[1] == 0)}
+
+
 def batched_mix(steps=30, nbox=64):
     """Batched form: `nbox` independent periodic boxes of uneven sizes (GLM and CT mixed),
     `steps` steps each with per-box CFL, in one graph-recorded persistent launch per solver
@@ -193,20 +246,7 @@ def batched_mix(steps=30, nbox=64):
     import pmfmhd
     specs = ics.batch_mix(nbox)
 
-    def build():
-        states = []
-        for sp in specs:
-            n = sp["n"]
-            b = ics.turbulent_box(n, seed=sp["seed"], beta=sp["beta"], b_index=sp["b_index"], kc=sp["kc"],
-                                  with_ct=sp["ct"])
-            s = pmfmhd.set_fields(pmfmhd.allocate_state((n, n, n), 1.0 / n, mhd_solver="ct" if sp["ct"] else "glm"),
-                                  b["U"])
-            if sp["ct"]:
-                pmfmhd.ct_faces_from_potential(s, *b["A_edge"])
-            states.append(s)
-        return states
-
-    states = build()
+    states = build_boxes(specs)
     # tiles per N and solver: the autotuner's choice on one box of each kind
     seen = set()
     for s, sp in zip(states, specs):
@@ -384,6 +424,8 @@ def main():
         del q
         if world == 1:
             extra["batched"] = batched_mix()
+        else:
+            extra["batched_sharded"] = sharded_batched_mix(rank, world)
     clocks = sampler.stop()
 
     if rank != 0:
