@@ -85,10 +85,11 @@ int pmfmhd_step_glm(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[
  * The GLM step of pmfmhd_step_glm on HOST buffers: Uh (9 host arrays) in, Unh (9 host arrays)
  * out, for a caller whose state lives in host memory (the reference's CPU-resident
  * `MHDState`, whose `step_ref!` this replaces for that case). The box is cut into `nchunks`
- * z-slabs (<= 0: 8; each at least 2 planes): slabs are copied in on one stream, stepped on a
+ * z-slabs (<= 0: 16; each at least 2 planes): slabs are copied in on one stream, stepped on a
  * second once their neighbours have arrived, and copied out on a third, so the PCIe traffic
  * both ways overlaps the compute. Pinned host memory (cudaHostAlloc / cudaHostRegister) is
- * needed for the overlap; pageable memory works, serialised. Ordered after the caller's
+ * needed for the overlap; pageable memory works, serialised. Nine arrays spaced one field
+ * apart (a (9, cells) block) move as one pitched copy per slab. Ordered after the caller's
  * stream; returns after Unh is complete. Device copies of the state are context workspace
  * (18 floats per cell, kept for the next call). No compensation (resid is not supported).
  */

@@ -376,7 +376,7 @@ int pmfmhd_step_glm_host(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const
   if (!nonnull(Uh, 9) || !nonnull(Unh, 9)) return PMFMHD_EINVAL;
   if (!std::isfinite(dt) || !std::isfinite(ch) || !std::isfinite(decay) || !(ch > 0.0f)) return PMFMHD_EINVAL;
   const int nz = g->nz;
-  int C = nchunks > 0 ? nchunks : 8;
+  int C = nchunks > 0 ? nchunks : 16;
   C = std::max(1, std::min(C, nz / 2));  // every chunk at least 2 planes: halos reach chunks c +- 1
   const long long nc = ncells(g), nxy = (long long)g->nx * g->ny;
   HostPath& hp = c->hp;
@@ -404,6 +404,14 @@ int pmfmhd_step_glm_host(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const
     Und[f] = hp.dev + (size_t)(9 + f) * nc;
   }
   auto zb = [&](int k) { return (int)((long long)nz * k / C); };  // chunk k = planes [zb(k), zb(k+1))
+  // host arrays laid out as one (9, cells) block move as one pitched copy per slab
+  auto uniform = [&](const float* const* p) {
+    for (int f = 1; f < 9; ++f)
+      if (p[f] != p[0] + (size_t)f * nc) return false;
+    return true;
+  };
+  const bool in2d = uniform(Uh), out2d = uniform(const_cast<const float* const*>(Unh));
+  const size_t pitch = (size_t)nc * sizeof(float);
   auto arrived = [&](int k) { return hp.ev[3 * k]; };
   auto computed = [&](int k) { return hp.ev[3 * k + 1]; };
   // ordered after the caller's prior work
@@ -415,9 +423,13 @@ int pmfmhd_step_glm_host(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const
   for (int i = 0; i < C; ++i) {
     const int k = (i == 0) ? C - 1 : i - 1;
     const size_t off = (size_t)zb(k) * nxy, len = (size_t)(zb(k + 1) - zb(k)) * nxy;
-    for (int f = 0; f < 9; ++f)
-      PMF_CK(cudaMemcpyAsync(const_cast<float*>(Ud[f]) + off, Uh[f] + off, len * sizeof(float),
-                             cudaMemcpyHostToDevice, sin));
+    if (in2d)
+      PMF_CK(cudaMemcpy2DAsync(const_cast<float*>(Ud[0]) + off, pitch, Uh[0] + off, pitch, len * sizeof(float), 9,
+                               cudaMemcpyHostToDevice, sin));
+    else
+      for (int f = 0; f < 9; ++f)
+        PMF_CK(cudaMemcpyAsync(const_cast<float*>(Ud[f]) + off, Uh[f] + off, len * sizeof(float),
+                               cudaMemcpyHostToDevice, sin));
     PMF_CK(cudaEventRecord(arrived(k), sin));
   }
   // compute chunk k once chunks k-1, k, k+1 (periodic) are resident; copy it out as soon as done
@@ -434,8 +446,12 @@ int pmfmhd_step_glm_host(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const
     PMF_CK(cudaEventRecord(computed(k), scomp));
     PMF_CK(cudaStreamWaitEvent(sout, computed(k), 0));
     const size_t off = (size_t)zb(k) * nxy, len = (size_t)(zb(k + 1) - zb(k)) * nxy;
-    for (int f = 0; f < 9; ++f)
-      PMF_CK(cudaMemcpyAsync(Unh[f] + off, Und[f] + off, len * sizeof(float), cudaMemcpyDeviceToHost, sout));
+    if (out2d)
+      PMF_CK(cudaMemcpy2DAsync(Unh[0] + off, pitch, Und[0] + off, pitch, len * sizeof(float), 9,
+                               cudaMemcpyDeviceToHost, sout));
+    else
+      for (int f = 0; f < 9; ++f)
+        PMF_CK(cudaMemcpyAsync(Unh[f] + off, Und[f] + off, len * sizeof(float), cudaMemcpyDeviceToHost, sout));
   }
   PMF_CK(cudaEventRecord(hp.ev[3 * (C - 1) + 2], sout));
   PMF_CK(cudaStreamWaitEvent(caller, hp.ev[3 * (C - 1) + 2], 0));

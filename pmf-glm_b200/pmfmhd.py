@@ -299,7 +299,7 @@ def step_cube(s: MHDState, dt: float, ch: float, decay: float) -> MHDState:
 
 
 def step_cube_host(s: MHDState, U_host: torch.Tensor, Unew_host: torch.Tensor, dt: float, ch: float, decay: float,
-                   nchunks: int = 8) -> None:
+                   nchunks: int = 16) -> None:
     """The GLM step on host (9, nc) float32 tensors (pinned for PCIe/compute overlap) with the
     grid and parameters of ``s`` (pmfmhd_step_glm_host); ``s``'s device fields are not used."""
     for t in (U_host, Unew_host):
