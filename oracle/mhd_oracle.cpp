@@ -147,7 +147,11 @@ template <class T> Q<T> hll_x(const Q<T>& L, const Q<T>& R, T g, T bn, T fbn, T 
 // glm_physics.jl:255-263
 template <class T> void hlld_star(T d, T u, T v, T w, T by, T bz, T S, T bn, T SM, T& ov, T& ow, T& oby, T& obz) {
   T denK = d * (S - u) * (S - SM) - bn * bn;
-  if (std::fabs(denK) < T(1e-12)) { ov = v; ow = w; oby = by; obz = bz; return; }
+  // The reference's degeneracy test is |denK| < 1e-12; it is widened here to |denK| <
+  // max(1e-12, 1e-5 bn^2), the FP32 rounding level of denK (a difference of two terms of
+  // size bn^2), as the device solver does: below it the single-star states are ~1/denK and the
+  // fan flux hinges on a 1-ulp cancellation.
+  if (std::fabs(denK) < mx(T(1e-12), T(1e-5) * bn * bn)) { ov = v; ow = w; oby = by; obz = bz; return; }
   T fac = bn * (SM - u) / denK;
   ov = v - by * fac; ow = w - bz * fac;
   oby = by * (d * (S - u) * (S - u) - bn * bn) / denK;

@@ -259,3 +259,27 @@ def test_tma_staged_interior_matches_oracle_and_status_is_clear():
         pmfmhd.step(dev, float(dt), ch=float(speed))
     assert not within_parity(cpu.U, pmfmhd.fields_to_host(dev))
     assert pmfmhd.device_status(dev) == 0
+
+
+def test_near_degenerate_hlld_face_stays_consistent():
+    """Regression: a 96^3 piece of the 512^3 turbulent box (seed 0) around a face where the
+    fast and Alfven speeds coincide to FP32 rounding. With the reference's absolute 1e-12
+    degeneracy test the single-star states reach ~1e4 and the fan flux rests on a 1-ulp
+    cancellation; the device step then diverged from the FP32 oracle after 12 steps. Both now
+    take the degenerate branch within 1e-5 B_n^2 and agree."""
+    import ics
+    n, m, c = 512, 96, (292, 205, 2)
+    U = ics.turbulent_box(n, seed=0)["U"].reshape(9, n, n, n)
+    zi, yi, xi = [(np.arange(m) + c[a] - m // 2) % n for a in (2, 1, 0)]
+    sub = np.ascontiguousarray(U[:, zi][:, :, yi][:, :, :, xi]).reshape(9, -1)
+    del U
+    dt, sp = 7.973075844347477e-05, 4.899301052093506
+    bcs = ("outflow",) * 3
+    dev = gpu_state(sub, (m, m, m), dx=1.0 / n, bcs=bcs)
+    cpu = oracle_state(sub, (m, m, m), dx=1.0 / n, bcs=bcs)
+    for _ in range(12):
+        pmfmhd.step(dev, dt, ch=sp)
+        cpu.step(dt, ch=sp)
+    host = pmfmhd.fields_to_host(dev)
+    assert np.isfinite(host).all()
+    assert not within_parity(cpu.U, host)
