@@ -182,6 +182,121 @@ def linf_vs_fp64(n=64, steps=20):
     return out
 
 
+def _field_stats(h, ref):
+    d = [np.abs(h[v].astype(np.float64) - ref[v]) / max(np.abs(ref[v]).max(), 1e-300) for v in range(8)]
+    return {"linf_rel_max": float(max(x.max() for x in d)), "p999_rel_max": float(max(np.quantile(x, 0.999) for x in d)),
+            "mean_rel_max": float(max(x.mean() for x in d))}
+
+
+def _accuracy_128(U, steps, label):
+    """GPU FP32 (plain and compensated) against the FP64 oracle on a 128^3 box, with the
+    oracle's own CFL dt sequence replayed on the GPU (so only arithmetic differs)."""
+    import oracle
+    import pmfmhd
+    n = int(round(U.shape[1] ** (1 / 3)))
+    ref = oracle.OracleState((n, n, n), 1 / n, dtype=np.float64)
+    ref.U[:] = U.astype(np.float64)
+    e0 = ref.conserved_totals()["energy"]
+    seq = []
+    for _ in range(steps):
+        dt, sp = ref.compute_dt(0.2)
+        ch = float(sp)
+        dte = float(dt) * float(sp) / max(float(sp), ch)
+        seq.append((dte, ch))
+        ref.step(dte, ch=ch)
+    out = {"case": label, "steps": steps, "n": n}
+    for comp in (False, True):
+        s = pmfmhd.set_fields(pmfmhd.allocate_state((n, n, n), 1 / n, compensated=comp), U)
+        for dte, ch in seq:
+            pmfmhd.step(s, dte, ch=ch)
+        h = pmfmhd.fields_to_host(s)
+        r = _field_stats(h, ref.U)
+        r["energy_ledger_drift"] = abs(pmfmhd.conserved_totals(s)["energy"] - e0) / abs(e0)
+        r["finite"] = bool(np.isfinite(h).all())
+        out["compensated" if comp else "plain"] = r
+        del s
+    return out
+
+
+def big_box_cases():
+    """The 512^3 configurations: precision form (plain vs compensated GLM, 20 fixed-dt steps,
+    FP64 ledger) and the stress case (Mach 3, beta 0.1, lognormal density with sigma 1,
+    P_B ~ k^2 cut at N/8; 40 compensated steps with the on-device CFL of the batch driver),
+    each with its FP64-oracle accuracy on 128^3 (the precision form's generator at 128^3;
+    the stress box averaged 4^3 -> 128^3)."""
+    import torch
+
+    import ics
+    import pmfmhd
+    n = 512
+    out = {}
+    box = ics.turbulent_box(n, seed=0)
+    U = box["U"]
+    del box
+    prec = {}
+    for comp in (False, True):
+        s = pmfmhd.set_fields(pmfmhd.allocate_state((n, n, n), 1 / n, compensated=comp), U)
+        pmfmhd.autotune(s)
+        pmfmhd.set_fields(s, U)
+        if comp:
+            for r in s.resid:
+                r.zero_()
+        e0 = pmfmhd.conserved_totals(s)["energy"]
+        dt, sp = pmfmhd.compute_dt(s, 0.2)
+        T = np.float32
+        decay = float(np.exp(T(T(-T(0.18) * T(sp) * T(dt)) / T(1 / n))))
+        pmfmhd.step_cube(s, dt, sp, decay)
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        for _ in range(20):
+            pmfmhd.step_cube(s, dt, sp, decay)
+        a1.record()
+        torch.cuda.synchronize()
+        ms = a0.elapsed_time(a1) / 20
+        prec["compensated" if comp else "plain"] = {
+            "value": n ** 3 / (ms / 1e3), "ms_per_step": ms,
+            "energy_ledger_drift_21_steps": abs(pmfmhd.conserved_totals(s)["energy"] - e0) / abs(e0)}
+        del s
+        torch.cuda.empty_cache()
+    del U
+    prec["accuracy_128"] = _accuracy_128(ics.turbulent_box(128, seed=0)["U"], 20, "precision-form generator at 128^3")
+    out["precision_512"] = prec
+    box = ics.turbulent_box(n, seed=0, mach=3.0, beta=0.1, rho_sigma=1.0, lognormal=True, kc=n / 8)
+    U = box["U"]
+    del box
+    s = pmfmhd.set_fields(pmfmhd.allocate_state((n, n, n), 1 / n, compensated=True), U)
+    pmfmhd.autotune(s)
+    pmfmhd.set_fields(s, U)
+    for r in s.resid:
+        r.zero_()
+    e0 = pmfmhd.conserved_totals(s)["energy"]
+    b = pmfmhd.Batch([s], cfl=0.2)
+    torch.cuda.synchronize()
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record()
+    b.step(40)
+    a1.record()
+    torch.cuda.synchronize()
+    ms = a0.elapsed_time(a1)
+    t, _, _ = b.query()
+    h = b.current_fields(0)
+    b.close()
+    brms = float(np.sqrt((h[5:8].astype(np.float64) ** 2).sum() / n ** 3))
+    stress = {"value": 40 * n ** 3 / (ms / 1e3), "ms_per_step": ms / 40, "t_end": float(t[0]),
+              "finite": bool(np.isfinite(h).all()), "rho_min": float(h[0].min()),
+              "energy_ledger_drift": abs(pmfmhd.conserved_totals(s)["energy"] - e0) / abs(e0)}
+    s2 = pmfmhd.set_fields(pmfmhd.allocate_state((n, n, n), 1 / n), h)
+    stress["divb_centred_dx_over_brms"] = pmfmhd.max_divb(s2) / n / brms
+    del s, s2, h
+    torch.cuda.empty_cache()
+    Ud = U.astype(np.float64).reshape(9, 128, 4, 128, 4, 128, 4).mean(axis=(2, 4, 6)).reshape(9, -1).astype(np.float32)
+    del U
+    stress["accuracy_128"] = _accuracy_128(Ud, 40, "stress box averaged 4^3 -> 128^3")
+    out["stress_512"] = stress
+    return out
+
+
 def build_boxes(specs):
     """Device states of the batched workload's boxes (host ICs from the seeded generator)."""
     import ics
@@ -424,6 +539,7 @@ def main():
         del q
         if world == 1:
             extra["batched"] = batched_mix()
+            extra["big_boxes"] = big_box_cases()
         else:
             extra["batched_sharded"] = sharded_batched_mix(rank, world)
     clocks = sampler.stop()
