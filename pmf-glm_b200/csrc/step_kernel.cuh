@@ -369,8 +369,22 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     return __ldg(a.face[D] + wrap1(pz, nz) * nxy + wrap1(y, ny) * nx + wrap1(x, nx));
   };
 
+  F9 Fx;  // this thread's lower x-face flux of the last owned plane solved
   for (int p = z0 - 1; p <= z1; ++p) {
-    __syncthreads();  // plane p+1 (converted during the previous pass) is in the ring
+    __syncthreads();  // plane p+1 (converted during the previous pass) is in the ring; the x/y
+                      // fluxes of plane p-1 are complete
+    // x/y flux divergence of plane p-1 for the owned rows, parked for its update in the z-solve
+    // of this pass (the face above lane 31 comes from the halo warp)
+    if (row_own && p > z0) {
+      F9 dxy;
+#pragma unroll
+      for (int i = 0; i < 9; ++i) {
+        const float dn = __shfl_down_sync(0xffffffffu, Fx[i], 1);
+        const float fxh = lane == TILE_X - 1 ? fxright[(w - 1) * 9 + i] : dn;
+        dxy[i] = (Fx[i] - fxh) + (fybuf[((w - 1) * 9 + i) * 32 + lane] - fybuf[(w * 9 + i) * 32 + lane]);
+      }
+      zc_store(18, dxy);
+    }
     const bool mid = p >= z0 && p < z1;  // an owned plane of this chunk
     const int cell_p = (mid && x < nx && y < ny) ? (p * nxy + y * nx + x) : 0;
     // this thread's Hancock state and face offsets of plane p, and (CT) its lower-face fields
@@ -494,7 +508,6 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     // ---- x-faces: lane l of a row warp solves the face below column l (lane 0 against the
     // left halo cell); the halo warp's right-side lanes solve the face above lane 31. Both
     // go through this one call site, so a face shared by two tiles gets the same bits.
-    F9 Fx;
     {
       F9 L, R = face_lo<RECON>(mh, ox);
       {
@@ -545,17 +558,6 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
           a.work[6][cell_p] = Fy[7];
         }
       }
-    }
-    __syncthreads();
-    if (row_own) {
-      F9 dxy;
-#pragma unroll
-      for (int i = 0; i < 9; ++i) {
-        const float dn = __shfl_down_sync(0xffffffffu, Fx[i], 1);
-        const float fxh = lane == TILE_X - 1 ? fxright[(w - 1) * 9 + i] : dn;
-        dxy[i] = (Fx[i] - fxh) + (fybuf[((w - 1) * 9 + i) * 32 + lane] - fybuf[(w * 9 + i) * 32 + lane]);
-      }
-      zc_store(18, dxy);
     }
   }
   cp_async_wait_all();
