@@ -39,6 +39,11 @@ template <int TY> __host__ __device__ constexpr int step_threads() { return 32 *
 // under half the SM's, registers capped at 128 per thread), so one CTA's barrier waits
 // overlap the other's work.
 template <int TY> __host__ __device__ constexpr int step_min_blocks() { return TY <= 5 ? 2 : 1; }
+// Registers per thread the compiler may use: each of the SM's four sub-partitions holds 16K
+// registers for the warps resident on it (ceil(warps / 4) per CTA times the CTAs per SM).
+template <int TY> __host__ __device__ constexpr int step_reg_cap() {
+  return 16384 / (32 * ((TY + 3 + 3) / 4) * step_min_blocks<TY>()) / 8 * 8;
+}
 
 // Number of CT workspace arrays written by the Godunov stage (reference CTState slots 4-15).
 constexpr int CT_NWORK = 12;
@@ -295,12 +300,28 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   // the columns/rows of a partial tile beyond the grid are periodic images)
   const int rad_xy = RAD ? (((y % ny) + ny) % ny) * nx + ((x % nx) + nx) % nx : 0;
 
-  // Conservative update of cell (x, y, pz) from its x/y divergence and its two z fluxes.
-  auto update_cell = [&](int pz, const F9& dxy, const F9& flo, const F9& fhi) {
+  // Where the register budget allows (TY = 8: three warps per sub-partition), the state and
+  // Kahan remainders of the next plane this thread updates are loaded one pass ahead, so their
+  // HBM/L2 latency overlaps a whole pass of flux work instead of stalling the update; under a
+  // 128-register cap the 16 extra live values would spill, and the update loads them itself.
+  constexpr bool PREFETCH = step_reg_cap<TY>() >= 160;
+  constexpr int NR = COMP ? (CT ? 4 : 7) : 1;
+  F9 u0;
+  float rk[NR];
+  auto prefetch_cell = [&](int pz) {
     const int c = pz * nxy + y * nx + x;
-    F9 u0;
 #pragma unroll
     for (int f = 0; f < 9; ++f) u0[f] = __ldg(a.U[f] + c);
+    if constexpr (COMP) {
+#pragma unroll
+      for (int i = 0; i < NR; ++i) rk[i] = a.resid[i][c];
+    }
+  };
+  // Conservative update of cell (x, y, pz) from its x/y divergence and its two z fluxes
+  // (u0 and rk hold that cell: loaded by prefetch_cell(pz) during the previous pass, or here).
+  auto update_cell = [&](int pz, const F9& dxy, const F9& flo, const F9& fhi) {
+    const int c = pz * nxy + y * nx + x;
+    if constexpr (!PREFETCH) prefetch_cell(pz);
     F9 un;
     float d[9];
 #pragma unroll
@@ -308,18 +329,14 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     un[0] = u0[0] + d[0];
     if constexpr (COMP) {
 #pragma unroll
-      for (int i = 1; i <= 4; ++i) {
-        float r = a.resid[i - 1][c];
+      for (int i = 1; i <= NR; ++i) {
+        float r = rk[i - 1];
         un[i] = comp_add(u0[i], d[i], r);
         a.resid[i - 1][c] = r;
       }
-      if constexpr (!CT) {
+      if constexpr (CT) {
 #pragma unroll
-        for (int i = 5; i <= 7; ++i) {
-          float r = a.resid[i - 1][c];
-          un[i] = comp_add(u0[i], d[i], r);
-          a.resid[i - 1][c] = r;
-        }
+        for (int i = NR + 1; i <= 7; ++i) un[i] = u0[i] + d[i];
       }
     } else {
 #pragma unroll
@@ -490,6 +507,9 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
         }
       }
       if (p > z0 && own) update_cell(p - 1, zc_load(18), zc_load(9), Fz);
+      if constexpr (PREFETCH) {
+        if (mid && own) prefetch_cell(p);
+      }
       zc_store(9, Fz);
     }
     }  // p > z0 - 1
