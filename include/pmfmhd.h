@@ -272,7 +272,7 @@ int pmfmhd_autotune(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[
 int pmfmhd_status(pmfmhd_ctx* ctx, int clear, void* stream);
 
 /* Pin (or query) the tile used for this grid/solver/mode on this context: `rows` owned rows
- * per CTA (an instantiated height: 5, 8, 10 or 13) and `planes` z-planes per CTA chunk. */
+ * per CTA (an instantiated height: 5, 8, 9, 10 or 13) and `planes` z-planes per CTA chunk. */
 int pmfmhd_set_tile(pmfmhd_ctx* ctx, const pmfmhd_grid* g, int mhd_solver, int compensated, int rows, int planes);
 int pmfmhd_get_tile(pmfmhd_ctx* ctx, const pmfmhd_grid* g, int mhd_solver, int compensated, int* rows,
                     int* planes);

@@ -214,12 +214,12 @@ __global__ void __launch_bounds__(kThreads) pmf_modes_kernel(const PmfModes P, f
 }
 
 // x <- x * mul (when `write`), partial[b] = sum of (x * mul)^2 over block b's cells (FP64)
-__global__ void __launch_bounds__(kThreads) scale_sumsq_kernel(float* __restrict__ x, long long n, float mul,
+__global__ void __launch_bounds__(kThreads) scale_sumsq_kernel(const float* src, float* x, long long n, float mul,
                                                                bool write, double* __restrict__ partial) {
   __shared__ double red[kThreads / 32];
   double acc = 0.0;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-    const float v = x[c] * mul;
+    const float v = src[c] * mul;
     if (write) x[c] = v;
     acc += (double)v * (double)v;
   }
@@ -495,10 +495,10 @@ int pmfmhd_pmf_batchelor_field(pmfmhd_ctx* c, const pmfmhd_pmf_params* p, float*
   PMF_CK(dsym.alloc(sym.size() * sizeof(float)));
   PMF_CK(cudaMemcpyAsync(dsym.p, sym.data(), sym.size() * sizeof(float), cudaMemcpyHostToDevice, s));
   PMF_CK(dbk.alloc(3 * (size_t)nck * sizeof(float2)));
-  if (preserve_low) {
-    PMF_CK(dlk.alloc(3 * (size_t)nck * sizeof(float2)));
-    PMF_CK(dtmp.alloc((size_t)n * sizeof(float)));
-  }
+  if (preserve_low) PMF_CK(dlk.alloc(3 * (size_t)nck * sizeof(float2)));
+  // cuFFT writes only to this scratch: its own allocation is aligned for the transform, while
+  // the caller's field arrays may sit at any float offset of a packed state
+  PMF_CK(dtmp.alloc((size_t)n * sizeof(float)));
   const int nb = blocks_for(n, c->sms);
   PMF_CK(dpart.alloc((size_t)nb * sizeof(double)));
   PMF_CK(dres.alloc(16 * sizeof(double)));
@@ -516,14 +516,14 @@ int pmfmhd_pmf_batchelor_field(pmfmhd_ctx* c, const pmfmhd_pmf_params* p, float*
   const float inv_n = (float)(1.0 / vt);  // FFTW's irfft is normalised
   double* res = static_cast<double*>(dres.p);
   double* part = static_cast<double*>(dpart.p);
+  float* tmp = static_cast<float*>(dtmp.p);
   for (int d = 0; d < 3; ++d) {
-    if ((rc = cufft_rc(cufftExecC2R(plan.h, reinterpret_cast<cufftComplex*>(bk + d * nck), B[d])))) return rc;
-    scale_sumsq_kernel<<<nb, kThreads, 0, s>>>(B[d], n, inv_n, true, part);
+    if ((rc = cufft_rc(cufftExecC2R(plan.h, reinterpret_cast<cufftComplex*>(bk + d * nck), tmp)))) return rc;
+    scale_sumsq_kernel<<<nb, kThreads, 0, s>>>(tmp, B[d], n, inv_n, true, part);
     fold_kernel<<<1, 1, 0, s>>>(part, nb, res, d);
     if (preserve_low) {
-      float* tmp = static_cast<float*>(dtmp.p);
       if ((rc = cufft_rc(cufftExecC2R(plan.h, reinterpret_cast<cufftComplex*>(lk + d * nck), tmp)))) return rc;
-      scale_sumsq_kernel<<<nb, kThreads, 0, s>>>(tmp, n, inv_n, false, part);
+      scale_sumsq_kernel<<<nb, kThreads, 0, s>>>(tmp, tmp, n, inv_n, false, part);
       fold_kernel<<<1, 1, 0, s>>>(part, nb, res, 3 + d);
     }
   }
@@ -537,7 +537,7 @@ int pmfmhd_pmf_batchelor_field(pmfmhd_ctx* c, const pmfmhd_pmf_params* p, float*
   if (!(ref_rms0 > 0.0)) return PMFMHD_EINADMISSIBLE;
   const float scale = (float)(p->brms / (norm == 2 ? ref_rms0 : rms0));
   for (int d = 0; d < 3; ++d) {
-    scale_sumsq_kernel<<<nb, kThreads, 0, s>>>(B[d], n, scale, true, part);
+    scale_sumsq_kernel<<<nb, kThreads, 0, s>>>(B[d], B[d], n, scale, true, part);
     fold_kernel<<<1, 1, 0, s>>>(part, nb, res, 6 + d);
   }
   PMF_CK(cudaGetLastError());
@@ -596,9 +596,10 @@ int pmfmhd_ct_faces_from_cells(pmfmhd_ctx* c, const pmfmhd_grid* g, float* const
     if (U[f] == nullptr) return PMFMHD_EINVAL;
   const int nx = g->nx, ny = g->ny, nz = g->nz, nxh = nx / 2 + 1;
   const long long n = ncells(g), nck = (long long)nxh * ny * nz;
+  const long long n2 = (n + 1) & ~1LL;  // component stride: every component 16-byte aligned for cuFFT
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   DevBuf dold, dbh, dface, dpart, dres;
-  PMF_CK(dold.alloc(3 * (size_t)n * sizeof(double)));
+  PMF_CK(dold.alloc(3 * (size_t)n2 * sizeof(double)));
   PMF_CK(dbh.alloc(3 * (size_t)nck * sizeof(double2)));
   PMF_CK(dface.alloc((size_t)n * sizeof(double)));
   const int nb = blocks_for(n, c->sms);
@@ -606,7 +607,7 @@ int pmfmhd_ct_faces_from_cells(pmfmhd_ctx* c, const pmfmhd_grid* g, float* const
   PMF_CK(dres.alloc(4 * sizeof(double)));
   double* old = static_cast<double*>(dold.p);
   double2* bh = static_cast<double2*>(dbh.p);
-  for (int d = 0; d < 3; ++d) to_double_kernel<<<nb, kThreads, 0, s>>>(U[5 + d], old + d * n, n);
+  for (int d = 0; d < 3; ++d) to_double_kernel<<<nb, kThreads, 0, s>>>(U[5 + d], old + d * n2, n);
   PMF_CK(cudaGetLastError());
   Plan fwd, inv;
   if ((rc = cufft_rc(cufftPlan3d(&fwd.h, nz, ny, nx, CUFFT_D2Z)))) return rc;
@@ -615,7 +616,7 @@ int pmfmhd_ct_faces_from_cells(pmfmhd_ctx* c, const pmfmhd_grid* g, float* const
   inv.ok = true;
   if ((rc = cufft_rc(cufftSetStream(fwd.h, s))) || (rc = cufft_rc(cufftSetStream(inv.h, s)))) return rc;
   for (int d = 0; d < 3; ++d)
-    if ((rc = cufft_rc(cufftExecD2Z(fwd.h, old + d * n, reinterpret_cast<cufftDoubleComplex*>(bh + d * nck)))))
+    if ((rc = cufft_rc(cufftExecD2Z(fwd.h, old + d * n2, reinterpret_cast<cufftDoubleComplex*>(bh + d * nck)))))
       return rc;
   ct_face_modes_kernel<<<blocks_for(nck, c->sms), kThreads, 0, s>>>(bh, nx, ny, nz);
   PMF_CK(cudaGetLastError());
@@ -627,7 +628,7 @@ int pmfmhd_ct_faces_from_cells(pmfmhd_ctx* c, const pmfmhd_grid* g, float* const
   PMF_CK(cudaGetLastError());
   if ((rc = pmfmhd_ct_install_faces(c, g, U, ct, stream))) return rc;
   double* part = static_cast<double*>(dpart.p);
-  ct_change_kernel<<<nb, kThreads, 0, s>>>(U[5], U[6], U[7], old, old + n, old + 2 * n, n, part);
+  ct_change_kernel<<<nb, kThreads, 0, s>>>(U[5], U[6], U[7], old, old + n2, old + 2 * n2, n, part);
   for (int q = 0; q < 3; ++q) fold_kernel<<<1, 1, 0, s>>>(part + q * nb, nb, static_cast<double*>(dres.p), q);
   PMF_CK(cudaGetLastError());
   double h[3];

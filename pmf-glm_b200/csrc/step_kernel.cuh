@@ -300,7 +300,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   // the columns/rows of a partial tile beyond the grid are periodic images)
   const int rad_xy = RAD ? (((y % ny) + ny) % ny) * nx + ((x % nx) + nx) % nx : 0;
 
-  // Where the register budget allows (TY = 8: three warps per sub-partition), the state and
+  // Where the register budget allows (TY = 8, 9: three warps per sub-partition), the state and
   // Kahan remainders of the next plane this thread updates are loaded one pass ahead, so their
   // HBM/L2 latency overlaps a whole pass of flux work instead of stalling the update; under a
   // 128-register cap the 16 extra live values would spill, and the update loads them itself.

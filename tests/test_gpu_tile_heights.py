@@ -1,0 +1,97 @@
+"""Every instantiated CTA tile height against the CPU oracle.
+
+The autotuner picks the tile height (owned rows per CTA) per grid, so each instantiation is a
+production path: each one steps a ragged periodic box (partial x/y tiles, a short last z
+chunk) in the GLM, compensated-GLM and CT forms, gated like test/test_backends.jl:65-121
+(per field max|cand-ref| <= 2e-6 + 5e-5*max|ref|).
+
+The smooth field of problems.jl:9-22 carries a uniform drift here: without it its mass flux is
+exactly zero by symmetry on a plane of faces, where the contact upwinding of the CT edge EMFs
+(ct.jl:57-66) takes the lower branch, the upper one or their mean on the sign of a rounding
+residue, so FP32 and FP64 runs (the oracle's own included) differ there by half the branch
+jump (By, Bz by 1.7e-5 and 3.7e-5 after four steps). The FP64 oracle is the reference."""
+import numpy as np
+import pytest
+
+import oracle
+import pmfmhd
+import problems
+from mhd_cases import within_parity
+
+pytestmark = pytest.mark.gpu
+
+TILE_ROWS = (5, 8, 9, 10, 13)
+DIMS = (37, 29, 11)
+
+
+def _drifting_field(dx, gamma=5 / 3, drift=(0.031, -0.017, 0.023)):
+    U = problems.turb_field(DIMS, dx).astype(np.float64)
+    rho, B = U[0], U[5:8]
+    v = U[1:4] / rho
+    p = (gamma - 1) * (U[4] - 0.5 * rho * (v ** 2).sum(0) - 0.5 * (B ** 2).sum(0))
+    v = v + np.array(drift)[:, None]
+    U[1:4] = rho * v
+    U[4] = p / (gamma - 1) + 0.5 * rho * (v ** 2).sum(0) + 0.5 * (B ** 2).sum(0)
+    return U.astype(np.float32)
+
+
+def _pair(mode):
+    dx = 1.0 / max(DIMS)
+    U = _drifting_field(dx)
+    kw = dict(compensated=True) if mode == "compensated" else {}
+    if mode == "ct":
+        kw = dict(mhd_solver="ct")
+    dev = pmfmhd.allocate_state(DIMS, dx, **kw)
+    pmfmhd.set_fields(dev, U)
+    if mode == "ct":
+        # odd extents: the FFT projection must not depend on even sizes or aligned fields
+        info = pmfmhd.ct_faces_from_cells(dev)
+        assert info["max_divb_face_dx_over_brms"] < 1e-5
+        U = pmfmhd.fields_to_host(dev)
+    cpu = oracle.OracleState(DIMS, dx, dtype=np.float64, **kw)
+    cpu.U[:] = U.astype(np.float64)
+    if mode == "ct":
+        nc = int(np.prod(DIMS))
+        cpu.faces[:] = dev.ct.packed[: 3 * nc].cpu().numpy().reshape(3, -1).astype(np.float64)
+    return dev, cpu
+
+
+@pytest.mark.parametrize("mode", ["glm", "compensated", "ct"])
+@pytest.mark.parametrize("rows", TILE_ROWS)
+def test_tile_height_matches_oracle(rows, mode):
+    dev, cpu = _pair(mode)
+    pmfmhd.set_tile(dev, rows, 8)
+    assert pmfmhd.get_tile(dev) == (rows, 8)
+    dt, speed = cpu.compute_dt(0.2)
+    for _ in range(4):
+        if mode == "ct":
+            cpu.step(dt)
+            pmfmhd.step(dev, float(dt), integrator="ref")
+        else:
+            cpu.step(dt, ch=speed)
+            pmfmhd.step(dev, float(dt), ch=float(speed))
+    host = pmfmhd.fields_to_host(dev)
+    assert not within_parity(cpu.U, host)
+    if mode == "ct":
+        nc = int(np.prod(DIMS))
+        faces = dev.ct.packed[: 3 * nc].cpu().numpy().reshape(3, -1)
+        for d in range(3):
+            assert np.abs(faces[d] - cpu.faces[d]).max() <= 2e-6 + 5e-5 * np.abs(cpu.faces[d]).max()
+
+
+def test_tile_heights_agree_to_rounding():
+    """The tile height changes which CTA computes a face, not the scheme: the heights agree
+    with each other to FP32 rounding (the instantiations may contract multiply-adds
+    differently, so bitwise equality is not required)."""
+    outs = []
+    for rows in TILE_ROWS:
+        dev, cpu = _pair("glm")
+        pmfmhd.set_tile(dev, rows, 8)
+        dt, speed = cpu.compute_dt(0.2)
+        dt, speed = np.float32(dt), np.float32(speed)
+        for _ in range(2):
+            pmfmhd.step(dev, float(dt), ch=float(speed))
+        outs.append(pmfmhd.fields_to_host(dev).astype(np.float64))
+    for o in outs[1:]:
+        for f in range(8):
+            assert np.abs(o[f] - outs[0][f]).max() <= 1e-6 * np.abs(outs[0][f]).max()
