@@ -37,7 +37,39 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--quick", action="store_true", help="skip the secondary measurements")
+    ap.add_argument("--ct-only", action="store_true",
+                    help="time only the constrained-transport step of the --n box (for kernel profiling)")
     return ap.parse_args()
+
+
+def ct_only(args):
+    """The CT leg alone (faces from the edge potential, autotuned tile, --warmup then --steps
+    steps): one JSON line with its device time per step, for profiling the CT kernels."""
+    import torch
+
+    import ics
+    import pmfmhd
+    n = args.n
+    boxc = ics.turbulent_box(n, seed=0, with_ct=True)
+    c = pmfmhd.set_fields(pmfmhd.allocate_state((n, n, n), 1.0 / n, mhd_solver="ct"), boxc["U"])
+    pmfmhd.ct_faces_from_potential(c, *boxc["A_edge"])
+    dtc, _ = pmfmhd.compute_dt(c, 0.2)
+    pmfmhd.autotune(c)
+    for _ in range(args.warmup):
+        pmfmhd.step(c, dtc, integrator="ref")
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(args.steps):
+        pmfmhd.step(c, dtc, integrator="ref")
+    a1.record(stream)
+    torch.cuda.synchronize()
+    ms = a0.elapsed_time(a1) / args.steps
+    host = pmfmhd.fields_to_host(c)
+    print(json.dumps({"ct_only": True, "n": n, "steps": args.steps, "ms_per_step": ms,
+                      "value": n ** 3 / (ms / 1e3), "unit": UNIT, "tile": list(pmfmhd.get_tile(c)),
+                      "finite": bool(np.isfinite(host).all())}))
 
 
 def workload_config(n, steps):
@@ -421,6 +453,9 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.ct_only:
+        ct_only(args)
         return
     import torch
     import torch.distributed as dist

@@ -140,7 +140,10 @@ __device__ __forceinline__ float gs05(float Ea0, float Eam, float Eb0, float Ebm
 enum { CT_BXF = 0, CT_BYF, CT_BZF, CT_MFX, CT_MFY, CT_MFZ, CT_FXBY, CT_FXBZ, CT_FYBX, CT_FYBZ, CT_FZBX, CT_FZBY,
        CT_ECX, CT_ECY, CT_ECZ, CT_EX, CT_EY, CT_EZ, CT_RBX, CT_RBY, CT_RBZ, CT_NSLOT };
 
-// edge EMFs of cell c from the lower-face fluxes and cell EMFs (ct.jl:71-93)
+// edge EMFs of cell c from the lower-face fluxes and cell EMFs (ct.jl:71-93). The inputs are
+// read through the same buffer the EMFs are stored into, so all 36 loads are issued before the
+// first store: the compiler may not move a load above a store that could alias it, and three
+// load-compute-store rounds would cost three memory latencies per cell.
 __device__ __forceinline__ void ct_emf_cell(float* __restrict__ ct, int nx, int ny, int nz, int c) {
   const int nxy = nx * ny, nc = nxy * nz;
   const float* W = ct;
@@ -149,15 +152,24 @@ __device__ __forceinline__ void ct_emf_cell(float* __restrict__ ct, int nx, int 
   const int cim = k * nxy + j * nx + im, cjm = k * nxy + jm * nx + i, ckm = km * nxy + j * nx + i;
   const int cimjm = k * nxy + jm * nx + im, cjmkm = km * nxy + jm * nx + i, ckmim = km * nxy + j * nx + im;
   auto w = [&](int s, int x) { return __ldg(W + (size_t)s * nc + x); };
-  ct[(size_t)CT_EZ * nc + c] =
-      gs05(-w(CT_FXBY, c), -w(CT_FXBY, cjm), w(CT_FYBX, c), w(CT_FYBX, cim), w(CT_MFX, c), w(CT_MFX, cjm),
-           w(CT_MFY, c), w(CT_MFY, cim), w(CT_ECZ, c), w(CT_ECZ, cim), w(CT_ECZ, cjm), w(CT_ECZ, cimjm));
-  ct[(size_t)CT_EX * nc + c] =
-      gs05(-w(CT_FYBZ, c), -w(CT_FYBZ, ckm), w(CT_FZBY, c), w(CT_FZBY, cjm), w(CT_MFY, c), w(CT_MFY, ckm),
-           w(CT_MFZ, c), w(CT_MFZ, cjm), w(CT_ECX, c), w(CT_ECX, cjm), w(CT_ECX, ckm), w(CT_ECX, cjmkm));
-  ct[(size_t)CT_EY * nc + c] =
-      gs05(-w(CT_FZBX, c), -w(CT_FZBX, cim), w(CT_FXBZ, c), w(CT_FXBZ, ckm), w(CT_MFZ, c), w(CT_MFZ, cim),
-           w(CT_MFX, c), w(CT_MFX, ckm), w(CT_ECY, c), w(CT_ECY, ckm), w(CT_ECY, cim), w(CT_ECY, ckmim));
+  // z edge
+  const float z0 = -w(CT_FXBY, c), z1 = -w(CT_FXBY, cjm), z2 = w(CT_FYBX, c), z3 = w(CT_FYBX, cim);
+  const float z4 = w(CT_MFX, c), z5 = w(CT_MFX, cjm), z6 = w(CT_MFY, c), z7 = w(CT_MFY, cim);
+  const float z8 = w(CT_ECZ, c), z9 = w(CT_ECZ, cim), z10 = w(CT_ECZ, cjm), z11 = w(CT_ECZ, cimjm);
+  // x edge
+  const float x0 = -w(CT_FYBZ, c), x1 = -w(CT_FYBZ, ckm), x2 = w(CT_FZBY, c), x3 = w(CT_FZBY, cjm);
+  const float x4 = w(CT_MFY, ckm), x5 = w(CT_MFZ, c), x6 = w(CT_MFZ, cjm);
+  const float x7 = w(CT_ECX, c), x8 = w(CT_ECX, cjm), x9 = w(CT_ECX, ckm), x10 = w(CT_ECX, cjmkm);
+  // y edge
+  const float y0 = -w(CT_FZBX, c), y1 = -w(CT_FZBX, cim), y2 = w(CT_FXBZ, c), y3 = w(CT_FXBZ, ckm);
+  const float y4 = w(CT_MFZ, cim), y5 = w(CT_MFX, ckm);
+  const float y6 = w(CT_ECY, c), y7 = w(CT_ECY, ckm), y8 = w(CT_ECY, cim), y9 = w(CT_ECY, ckmim);
+  const float ez = gs05(z0, z1, z2, z3, z4, z5, z6, z7, z8, z9, z10, z11);
+  const float ex = gs05(x0, x1, x2, x3, z6, x4, x5, x6, x7, x8, x9, x10);
+  const float ey = gs05(y0, y1, y2, y3, x5, y4, z4, y5, y6, y7, y8, y9);
+  ct[(size_t)CT_EZ * nc + c] = ez;
+  ct[(size_t)CT_EX * nc + c] = ex;
+  ct[(size_t)CT_EY * nc + c] = ey;
 }
 
 static __global__ void __launch_bounds__(AUX_THREADS) ct_emf_kernel(float* __restrict__ ct, int nx, int ny, int nz) {
@@ -181,23 +193,24 @@ __device__ __forceinline__ void ct_face_cell(float* __restrict__ ct, int nx, int
   float* bxf = ct + (size_t)CT_BXF * nc;
   float* byf = ct + (size_t)CT_BYF * nc;
   float* bzf = ct + (size_t)CT_BZF * nc;
+  // every load before the first store (the faces, remainders and EMFs share one buffer)
+  const float fx = bxf[c], fy = byf[c], fz = bzf[c];
   if (COMP) {
     float* rbx = ct + (size_t)CT_RBX * nc;
     float* rby = ct + (size_t)CT_RBY * nc;
     float* rbz = ct + (size_t)CT_RBZ * nc;
-    float r = rbx[c];
-    bxf[c] = comp_add(bxf[c], -dbx, r);
-    rbx[c] = r;
-    r = rby[c];
-    byf[c] = comp_add(byf[c], -dby, r);
-    rby[c] = r;
-    r = rbz[c];
-    bzf[c] = comp_add(bzf[c], -dbz, r);
-    rbz[c] = r;
+    float rx = rbx[c], ry = rby[c], rz = rbz[c];
+    const float nbx = comp_add(fx, -dbx, rx), nby = comp_add(fy, -dby, ry), nbz = comp_add(fz, -dbz, rz);
+    bxf[c] = nbx;
+    byf[c] = nby;
+    bzf[c] = nbz;
+    rbx[c] = rx;
+    rby[c] = ry;
+    rbz[c] = rz;
   } else {
-    bxf[c] -= dbx;
-    byf[c] -= dby;
-    bzf[c] -= dbz;
+    bxf[c] = fx - dbx;
+    byf[c] = fy - dby;
+    bzf[c] = fz - dbz;
   }
 }
 
@@ -220,11 +233,14 @@ __device__ __forceinline__ float ct_bcc_cell(const float* __restrict__ ct, const
   const float bx = 0.5f * (bxf[c] + bxf[k * nxy + j * nx + wrap_inc(i, nx)]);
   const float by = 0.5f * (byf[c] + byf[k * nxy + wrap_inc(j, ny) * nx + i]);
   const float bz = 0.5f * (bzf[c] + bzf[wrap_inc(k, nz) * nxy + j * nx + i]);
+  // the hydro fields are read before the B stores (all nine fields may share one buffer)
+  F9 u{{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, bx, by, bz, 0.0f}};
+  if (want_speed)
+    for (int f = 0; f < 5; ++f) u[f] = Un.p[f][c];
   Un.p[5][c] = bx;
   Un.p[6][c] = by;
   Un.p[7][c] = bz;
   if (!want_speed) return 0.0f;
-  F9 u{{Un.p[0][c], Un.p[1][c], Un.p[2][c], Un.p[3][c], Un.p[4][c], bx, by, bz, 0.0f}};
   return cell_wavespeed(u, P);
 }
 
