@@ -172,11 +172,6 @@ __device__ __forceinline__ void ct_emf_cell(float* __restrict__ ct, int nx, int 
   ct[(size_t)CT_EY * nc + c] = ey;
 }
 
-static __global__ void __launch_bounds__(AUX_THREADS) ct_emf_kernel(float* __restrict__ ct, int nx, int ny, int nz) {
-  const int nc = nx * ny * nz;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) ct_emf_cell(ct, nx, ny, nz, c);
-}
-
 // face update of cell c by the discrete curl of the edge EMFs, plain or Kahan (ct.jl:96-129)
 template <bool COMP>
 __device__ __forceinline__ void ct_face_cell(float* __restrict__ ct, int nx, int ny, int nz, float dtdx, int c) {
@@ -214,14 +209,6 @@ __device__ __forceinline__ void ct_face_cell(float* __restrict__ ct, int nx, int
   }
 }
 
-template <bool COMP>
-static __global__ void __launch_bounds__(AUX_THREADS) ct_face_kernel(float* __restrict__ ct, int nx, int ny, int nz,
-                                                              float dtdx) {
-  const int nc = nx * ny * nz;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
-    ct_face_cell<COMP>(ct, nx, ny, nz, dtdx, c);
-}
-
 // cell B of cell c = face average (ct.jl:132-143); returns the new state's signal speed
 __device__ __forceinline__ float ct_bcc_cell(const float* __restrict__ ct, const MPtr9& Un, int nx, int ny, int nz,
                                              const Phys& P, bool want_speed, int c) {
@@ -244,12 +231,121 @@ __device__ __forceinline__ float ct_bcc_cell(const float* __restrict__ ct, const
   return cell_wavespeed(u, P);
 }
 
-static __global__ void __launch_bounds__(AUX_THREADS) ct_bcc_kernel(const float* __restrict__ ct, const MPtr9 Un, int nx,
-                                                             int ny, int nz, Phys P, unsigned int* smax_bits) {
-  const int nc = nx * ny * nz;
+// ---- column forms of the CT companion kernels (one box) ---------------------------------
+// One thread per (x, y) column of a 32 x 8 tile marches a chunk of CTC_Z planes in z: the
+// cell index needs no division, every slot has its own restrict pointer (so the compiler
+// may overlap one plane's loads with the last plane's stores), and the values of plane k
+// that plane k+1 reads again as its lower neighbour stay in registers (25 loads per cell
+// for the EMFs instead of 36). The arithmetic per cell is that of ct_emf_cell,
+// ct_face_cell and ct_bcc_cell.
+constexpr int CTC_X = 32, CTC_Y = AUX_THREADS / 32, CTC_Z = 16;
+inline dim3 ctc_grid(int nx, int ny, int nz) {
+  return dim3((nx + CTC_X - 1) / CTC_X, (ny + CTC_Y - 1) / CTC_Y, (nz + CTC_Z - 1) / CTC_Z);
+}
+
+// edge EMFs (ct.jl:71-93)
+static __global__ void __launch_bounds__(AUX_THREADS) ct_emf_col_kernel(
+    const float* __restrict__ MFX, const float* __restrict__ MFY, const float* __restrict__ MFZ,
+    const float* __restrict__ FXBY, const float* __restrict__ FXBZ, const float* __restrict__ FYBX,
+    const float* __restrict__ FYBZ, const float* __restrict__ FZBX, const float* __restrict__ FZBY,
+    const float* __restrict__ ECX, const float* __restrict__ ECY, const float* __restrict__ ECZ,
+    float* __restrict__ EX, float* __restrict__ EY, float* __restrict__ EZ, int nx, int ny, int nz) {
+  const int i = blockIdx.x * CTC_X + (threadIdx.x & 31), j = blockIdx.y * CTC_Y + (threadIdx.x >> 5);
+  if (i >= nx || j >= ny) return;
+  const int z0 = blockIdx.z * CTC_Z, z1 = min(z0 + CTC_Z, nz);
+  const size_t nxy = (size_t)nx * ny;
+  const int im = wrap_dec(i, nx), jm = wrap_dec(j, ny);
+  const size_t o = (size_t)j * nx + i, oim = (size_t)j * nx + im, ojm = (size_t)jm * nx + i,
+               oimjm = (size_t)jm * nx + im;
+  // plane k-1 values of the x and y edges
+  size_t b = (size_t)wrap_dec(z0, nz) * nxy;
+  float pFYBZ = FYBZ[b + o], pMFY = MFY[b + o], pECX = ECX[b + o], pECXjm = ECX[b + ojm];
+  float pFXBZ = FXBZ[b + o], pMFX = MFX[b + o], pECY = ECY[b + o], pECYim = ECY[b + oim];
+  for (int k = z0; k < z1; ++k) {
+    b = (size_t)k * nxy;
+    const float fxby = FXBY[b + o], fxby_jm = FXBY[b + ojm], fybx = FYBX[b + o], fybx_im = FYBX[b + oim];
+    const float mfx = MFX[b + o], mfx_jm = MFX[b + ojm], mfy = MFY[b + o], mfy_im = MFY[b + oim];
+    const float ecz = ECZ[b + o], ecz_im = ECZ[b + oim], ecz_jm = ECZ[b + ojm], ecz_imjm = ECZ[b + oimjm];
+    const float fybz = FYBZ[b + o], fzby = FZBY[b + o], fzby_jm = FZBY[b + ojm], mfz = MFZ[b + o];
+    const float mfz_jm = MFZ[b + ojm], ecx = ECX[b + o], ecx_jm = ECX[b + ojm];
+    const float fzbx = FZBX[b + o], fzbx_im = FZBX[b + oim], fxbz = FXBZ[b + o], mfz_im = MFZ[b + oim];
+    const float ecy = ECY[b + o], ecy_im = ECY[b + oim];
+    EZ[b + o] = gs05(-fxby, -fxby_jm, fybx, fybx_im, mfx, mfx_jm, mfy, mfy_im, ecz, ecz_im, ecz_jm, ecz_imjm);
+    EX[b + o] = gs05(-fybz, -pFYBZ, fzby, fzby_jm, mfy, pMFY, mfz, mfz_jm, ecx, ecx_jm, pECX, pECXjm);
+    EY[b + o] = gs05(-fzbx, -fzbx_im, fxbz, pFXBZ, mfz, mfz_im, mfx, pMFX, ecy, pECY, ecy_im, pECYim);
+    pFYBZ = fybz; pMFY = mfy; pECX = ecx; pECXjm = ecx_jm;
+    pFXBZ = fxbz; pMFX = mfx; pECY = ecy; pECYim = ecy_im;
+  }
+}
+
+// face update by the discrete curl of the edge EMFs, plain or Kahan (ct.jl:96-129)
+template <bool COMP>
+static __global__ void __launch_bounds__(AUX_THREADS) ct_face_col_kernel(
+    const float* __restrict__ ex, const float* __restrict__ ey, const float* __restrict__ ez,
+    float* __restrict__ bxf, float* __restrict__ byf, float* __restrict__ bzf, float* __restrict__ rbx,
+    float* __restrict__ rby, float* __restrict__ rbz, int nx, int ny, int nz, float dtdx) {
+  const int i = blockIdx.x * CTC_X + (threadIdx.x & 31), j = blockIdx.y * CTC_Y + (threadIdx.x >> 5);
+  if (i >= nx || j >= ny) return;
+  const int z0 = blockIdx.z * CTC_Z, z1 = min(z0 + CTC_Z, nz);
+  const size_t nxy = (size_t)nx * ny;
+  const size_t o = (size_t)j * nx + i, oip = (size_t)j * nx + wrap_inc(i, nx), ojp = (size_t)wrap_inc(j, ny) * nx + i;
+  // plane k values that plane k-1 read as its upper neighbour
+  float ex_c = ex[(size_t)z0 * nxy + o], ey_c = ey[(size_t)z0 * nxy + o];
+  for (int k = z0; k < z1; ++k) {
+    const size_t b = (size_t)k * nxy, bp = (size_t)wrap_inc(k, nz) * nxy;
+    const float ez_c = ez[b + o], ez_jp = ez[b + ojp], ez_ip = ez[b + oip], ey_ip = ey[b + oip], ex_jp = ex[b + ojp];
+    const float ey_kp = ey[bp + o], ex_kp = ex[bp + o];
+    const float dbx = dtdx * ((ez_jp - ez_c) - (ey_kp - ey_c));
+    const float dby = dtdx * ((ex_kp - ex_c) - (ez_ip - ez_c));
+    const float dbz = dtdx * ((ey_ip - ey_c) - (ex_jp - ex_c));
+    const float fx = bxf[b + o], fy = byf[b + o], fz = bzf[b + o];
+    if (COMP) {
+      float rx = rbx[b + o], ry = rby[b + o], rz = rbz[b + o];
+      const float nbx = comp_add(fx, -dbx, rx), nby = comp_add(fy, -dby, ry), nbz = comp_add(fz, -dbz, rz);
+      bxf[b + o] = nbx;
+      byf[b + o] = nby;
+      bzf[b + o] = nbz;
+      rbx[b + o] = rx;
+      rby[b + o] = ry;
+      rbz[b + o] = rz;
+    } else {
+      bxf[b + o] = fx - dbx;
+      byf[b + o] = fy - dby;
+      bzf[b + o] = fz - dbz;
+    }
+    ex_c = ex_kp;
+    ey_c = ey_kp;
+  }
+}
+
+// cell B = face average (ct.jl:132-143) and the new state's signal speed
+static __global__ void __launch_bounds__(AUX_THREADS) ct_bcc_col_kernel(
+    const float* __restrict__ bxf, const float* __restrict__ byf, const float* __restrict__ bzf, const MPtr9 Un,
+    int nx, int ny, int nz, Phys P, unsigned int* smax_bits) {
+  const int i = blockIdx.x * CTC_X + (threadIdx.x & 31), j = blockIdx.y * CTC_Y + (threadIdx.x >> 5);
   float m = 0.0f;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
-    m = fmaxf(m, ct_bcc_cell(ct, Un, nx, ny, nz, P, smax_bits != nullptr, c));
+  if (i < nx && j < ny) {  // no early return: every thread joins the block reduction
+    const int z0 = blockIdx.z * CTC_Z, z1 = min(z0 + CTC_Z, nz);
+    const size_t nxy = (size_t)nx * ny;
+    const size_t o = (size_t)j * nx + i, oip = (size_t)j * nx + wrap_inc(i, nx),
+                 ojp = (size_t)wrap_inc(j, ny) * nx + i;
+    float bz_c = bzf[(size_t)z0 * nxy + o];
+    for (int k = z0; k < z1; ++k) {
+      const size_t b = (size_t)k * nxy, c = b + o;
+      const float bz_kp = bzf[(size_t)wrap_inc(k, nz) * nxy + o];
+      const float bx = 0.5f * (bxf[c] + bxf[b + oip]);
+      const float by = 0.5f * (byf[c] + byf[b + ojp]);
+      const float bz = 0.5f * (bz_c + bz_kp);
+      F9 u{{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, bx, by, bz, 0.0f}};
+      if (smax_bits != nullptr)
+        for (int f = 0; f < 5; ++f) u[f] = Un.p[f][c];
+      Un.p[5][c] = bx;
+      Un.p[6][c] = by;
+      Un.p[7][c] = bz;
+      if (smax_bits != nullptr) m = fmaxf(m, cell_wavespeed(u, P));
+      bz_c = bz_kp;
+    }
+  }
   if (smax_bits != nullptr) {
     m = block_reduce_max(m);
     if (threadIdx.x == 0) atomicMax(smax_bits, __float_as_uint(m));

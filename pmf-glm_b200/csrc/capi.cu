@@ -255,14 +255,25 @@ int enqueue_ct(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], flo
   for (int k = 0; k < CT_NWORK; ++k) a.work[k] = ct + (size_t)(CT_MFX + k) * nc;
   int rc = launch_step(c, g, a, tune_for(c, g, true, comp), true, comp, s, st ? st->src : SRC_NONE);
   if (rc != PMFMHD_OK) return rc;
-  const int nb = aux_blocks(c, nc);
-  ct_emf_kernel<<<nb, AUX_THREADS, 0, s>>>(ct, g->nx, g->ny, g->nz);
-  if (comp_faces) ct_face_kernel<true><<<nb, AUX_THREADS, 0, s>>>(ct, g->nx, g->ny, g->nz, dtdx);
-  else ct_face_kernel<false><<<nb, AUX_THREADS, 0, s>>>(ct, g->nx, g->ny, g->nz, dtdx);
+  auto sl = [&](int k) { return ct + (size_t)k * nc; };
+  const dim3 cg = ctc_grid(g->nx, g->ny, g->nz);
+  ct_emf_col_kernel<<<cg, AUX_THREADS, 0, s>>>(sl(CT_MFX), sl(CT_MFY), sl(CT_MFZ), sl(CT_FXBY), sl(CT_FXBZ),
+                                               sl(CT_FYBX), sl(CT_FYBZ), sl(CT_FZBX), sl(CT_FZBY), sl(CT_ECX),
+                                               sl(CT_ECY), sl(CT_ECZ), sl(CT_EX), sl(CT_EY), sl(CT_EZ), g->nx,
+                                               g->ny, g->nz);
+  if (comp_faces)
+    ct_face_col_kernel<true><<<cg, AUX_THREADS, 0, s>>>(sl(CT_EX), sl(CT_EY), sl(CT_EZ), sl(CT_BXF), sl(CT_BYF),
+                                                        sl(CT_BZF), sl(CT_RBX), sl(CT_RBY), sl(CT_RBZ), g->nx,
+                                                        g->ny, g->nz, dtdx);
+  else
+    ct_face_col_kernel<false><<<cg, AUX_THREADS, 0, s>>>(sl(CT_EX), sl(CT_EY), sl(CT_EZ), sl(CT_BXF), sl(CT_BYF),
+                                                         sl(CT_BZF), sl(CT_RBX), sl(CT_RBY), sl(CT_RBZ), g->nx,
+                                                         g->ny, g->nz, dtdx);
   PMF_CK(cudaMemsetAsync(c->d_smax, 0, sizeof(unsigned int), s));
   MPtr9 un;
   for (int f = 0; f < 9; ++f) un.p[f] = Un[f];
-  ct_bcc_kernel<<<nb, AUX_THREADS, 0, s>>>(ct, un, g->nx, g->ny, g->nz, phys_of(g), c->d_smax);
+  ct_bcc_col_kernel<<<cg, AUX_THREADS, 0, s>>>(sl(CT_BXF), sl(CT_BYF), sl(CT_BZF), un, g->nx, g->ny, g->nz,
+                                               phys_of(g), c->d_smax);
   PMF_CK(cudaGetLastError());
   return PMFMHD_OK;
 }
