@@ -140,119 +140,33 @@ __device__ __forceinline__ float gs05(float Ea0, float Eam, float Eb0, float Ebm
 enum { CT_BXF = 0, CT_BYF, CT_BZF, CT_MFX, CT_MFY, CT_MFZ, CT_FXBY, CT_FXBZ, CT_FYBX, CT_FYBZ, CT_FZBX, CT_FZBY,
        CT_ECX, CT_ECY, CT_ECZ, CT_EX, CT_EY, CT_EZ, CT_RBX, CT_RBY, CT_RBZ, CT_NSLOT };
 
-// edge EMFs of cell c from the lower-face fluxes and cell EMFs (ct.jl:71-93). The inputs are
-// read through the same buffer the EMFs are stored into, so all 36 loads are issued before the
-// first store: the compiler may not move a load above a store that could alias it, and three
-// load-compute-store rounds would cost three memory latencies per cell.
-__device__ __forceinline__ void ct_emf_cell(float* __restrict__ ct, int nx, int ny, int nz, int c) {
-  const int nxy = nx * ny, nc = nxy * nz;
-  const float* W = ct;
-  const int i = c % nx, j = (c / nx) % ny, k = c / nxy;
-  const int im = wrap_dec(i, nx), jm = wrap_dec(j, ny), km = wrap_dec(k, nz);
-  const int cim = k * nxy + j * nx + im, cjm = k * nxy + jm * nx + i, ckm = km * nxy + j * nx + i;
-  const int cimjm = k * nxy + jm * nx + im, cjmkm = km * nxy + jm * nx + i, ckmim = km * nxy + j * nx + im;
-  auto w = [&](int s, int x) { return __ldg(W + (size_t)s * nc + x); };
-  // z edge
-  const float z0 = -w(CT_FXBY, c), z1 = -w(CT_FXBY, cjm), z2 = w(CT_FYBX, c), z3 = w(CT_FYBX, cim);
-  const float z4 = w(CT_MFX, c), z5 = w(CT_MFX, cjm), z6 = w(CT_MFY, c), z7 = w(CT_MFY, cim);
-  const float z8 = w(CT_ECZ, c), z9 = w(CT_ECZ, cim), z10 = w(CT_ECZ, cjm), z11 = w(CT_ECZ, cimjm);
-  // x edge
-  const float x0 = -w(CT_FYBZ, c), x1 = -w(CT_FYBZ, ckm), x2 = w(CT_FZBY, c), x3 = w(CT_FZBY, cjm);
-  const float x4 = w(CT_MFY, ckm), x5 = w(CT_MFZ, c), x6 = w(CT_MFZ, cjm);
-  const float x7 = w(CT_ECX, c), x8 = w(CT_ECX, cjm), x9 = w(CT_ECX, ckm), x10 = w(CT_ECX, cjmkm);
-  // y edge
-  const float y0 = -w(CT_FZBX, c), y1 = -w(CT_FZBX, cim), y2 = w(CT_FXBZ, c), y3 = w(CT_FXBZ, ckm);
-  const float y4 = w(CT_MFZ, cim), y5 = w(CT_MFX, ckm);
-  const float y6 = w(CT_ECY, c), y7 = w(CT_ECY, ckm), y8 = w(CT_ECY, cim), y9 = w(CT_ECY, ckmim);
-  const float ez = gs05(z0, z1, z2, z3, z4, z5, z6, z7, z8, z9, z10, z11);
-  const float ex = gs05(x0, x1, x2, x3, z6, x4, x5, x6, x7, x8, x9, x10);
-  const float ey = gs05(y0, y1, y2, y3, x5, y4, z4, y5, y6, y7, y8, y9);
-  ct[(size_t)CT_EZ * nc + c] = ez;
-  ct[(size_t)CT_EX * nc + c] = ex;
-  ct[(size_t)CT_EY * nc + c] = ey;
-}
-
-// face update of cell c by the discrete curl of the edge EMFs, plain or Kahan (ct.jl:96-129)
-template <bool COMP>
-__device__ __forceinline__ void ct_face_cell(float* __restrict__ ct, int nx, int ny, int nz, float dtdx, int c) {
-  const int nxy = nx * ny, nc = nxy * nz;
-  const float* ex = ct + (size_t)CT_EX * nc;
-  const float* ey = ct + (size_t)CT_EY * nc;
-  const float* ez = ct + (size_t)CT_EZ * nc;
-  const int i = c % nx, j = (c / nx) % ny, k = c / nxy;
-  const int ip = k * nxy + j * nx + wrap_inc(i, nx), jp = k * nxy + wrap_inc(j, ny) * nx + i,
-            kp = wrap_inc(k, nz) * nxy + j * nx + i;
-  const float dbx = dtdx * ((ez[jp] - ez[c]) - (ey[kp] - ey[c]));
-  const float dby = dtdx * ((ex[kp] - ex[c]) - (ez[ip] - ez[c]));
-  const float dbz = dtdx * ((ey[ip] - ey[c]) - (ex[jp] - ex[c]));
-  float* bxf = ct + (size_t)CT_BXF * nc;
-  float* byf = ct + (size_t)CT_BYF * nc;
-  float* bzf = ct + (size_t)CT_BZF * nc;
-  // every load before the first store (the faces, remainders and EMFs share one buffer)
-  const float fx = bxf[c], fy = byf[c], fz = bzf[c];
-  if (COMP) {
-    float* rbx = ct + (size_t)CT_RBX * nc;
-    float* rby = ct + (size_t)CT_RBY * nc;
-    float* rbz = ct + (size_t)CT_RBZ * nc;
-    float rx = rbx[c], ry = rby[c], rz = rbz[c];
-    const float nbx = comp_add(fx, -dbx, rx), nby = comp_add(fy, -dby, ry), nbz = comp_add(fz, -dbz, rz);
-    bxf[c] = nbx;
-    byf[c] = nby;
-    bzf[c] = nbz;
-    rbx[c] = rx;
-    rby[c] = ry;
-    rbz[c] = rz;
-  } else {
-    bxf[c] = fx - dbx;
-    byf[c] = fy - dby;
-    bzf[c] = fz - dbz;
-  }
-}
-
-// cell B of cell c = face average (ct.jl:132-143); returns the new state's signal speed
-__device__ __forceinline__ float ct_bcc_cell(const float* __restrict__ ct, const MPtr9& Un, int nx, int ny, int nz,
-                                             const Phys& P, bool want_speed, int c) {
-  const int nxy = nx * ny, nc = nxy * nz;
-  const float* bxf = ct + (size_t)CT_BXF * nc;
-  const float* byf = ct + (size_t)CT_BYF * nc;
-  const float* bzf = ct + (size_t)CT_BZF * nc;
-  const int i = c % nx, j = (c / nx) % ny, k = c / nxy;
-  const float bx = 0.5f * (bxf[c] + bxf[k * nxy + j * nx + wrap_inc(i, nx)]);
-  const float by = 0.5f * (byf[c] + byf[k * nxy + wrap_inc(j, ny) * nx + i]);
-  const float bz = 0.5f * (bzf[c] + bzf[wrap_inc(k, nz) * nxy + j * nx + i]);
-  // the hydro fields are read before the B stores (all nine fields may share one buffer)
-  F9 u{{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, bx, by, bz, 0.0f}};
-  if (want_speed)
-    for (int f = 0; f < 5; ++f) u[f] = Un.p[f][c];
-  Un.p[5][c] = bx;
-  Un.p[6][c] = by;
-  Un.p[7][c] = bz;
-  if (!want_speed) return 0.0f;
-  return cell_wavespeed(u, P);
-}
-
-// ---- column forms of the CT companion kernels (one box) ---------------------------------
+// ---- CT companion kernels: column forms -------------------------------------------------
 // One thread per (x, y) column of a 32 x 8 tile marches a chunk of CTC_Z planes in z: the
 // cell index needs no division, every slot has its own restrict pointer (so the compiler
 // may overlap one plane's loads with the last plane's stores), and the values of plane k
 // that plane k+1 reads again as its lower neighbour stay in registers (25 loads per cell
-// for the EMFs instead of 36). The arithmetic per cell is that of ct_emf_cell,
-// ct_face_cell and ct_bcc_cell.
+// for the EMFs, of the 36 values its stencil touches). Per cell: the Gardiner & Stone EMFs (ct.jl:71-93), the face
+// update (ct.jl:96-129) and the face-average cell B (ct.jl:132-143).
 constexpr int CTC_X = 32, CTC_Y = AUX_THREADS / 32, CTC_Z = 16;
 inline dim3 ctc_grid(int nx, int ny, int nz) {
   return dim3((nx + CTC_X - 1) / CTC_X, (ny + CTC_Y - 1) / CTC_Y, (nz + CTC_Z - 1) / CTC_Z);
 }
 
+// The column bodies: tile (tx, ty), z chunk tz; thread t of AUX_THREADS owns column
+// (tx*32 + t%32, ty*CTC_Y + t/32). Used by the single-box kernels below and by the batched
+// driver, which maps its blocks to (box, tile).
+
 // edge EMFs (ct.jl:71-93)
-static __global__ void __launch_bounds__(AUX_THREADS) ct_emf_col_kernel(
+__device__ __forceinline__ void ct_emf_col(
     const float* __restrict__ MFX, const float* __restrict__ MFY, const float* __restrict__ MFZ,
     const float* __restrict__ FXBY, const float* __restrict__ FXBZ, const float* __restrict__ FYBX,
     const float* __restrict__ FYBZ, const float* __restrict__ FZBX, const float* __restrict__ FZBY,
     const float* __restrict__ ECX, const float* __restrict__ ECY, const float* __restrict__ ECZ,
-    float* __restrict__ EX, float* __restrict__ EY, float* __restrict__ EZ, int nx, int ny, int nz) {
-  const int i = blockIdx.x * CTC_X + (threadIdx.x & 31), j = blockIdx.y * CTC_Y + (threadIdx.x >> 5);
+    float* __restrict__ EX, float* __restrict__ EY, float* __restrict__ EZ, int nx, int ny, int nz, int tx, int ty,
+    int tz) {
+  const int i = tx * CTC_X + (threadIdx.x & 31), j = ty * CTC_Y + (threadIdx.x >> 5);
   if (i >= nx || j >= ny) return;
-  const int z0 = blockIdx.z * CTC_Z, z1 = min(z0 + CTC_Z, nz);
+  const int z0 = tz * CTC_Z, z1 = min(z0 + CTC_Z, nz);
   const size_t nxy = (size_t)nx * ny;
   const int im = wrap_dec(i, nx), jm = wrap_dec(j, ny);
   const size_t o = (size_t)j * nx + i, oim = (size_t)j * nx + im, ojm = (size_t)jm * nx + i,
@@ -280,13 +194,14 @@ static __global__ void __launch_bounds__(AUX_THREADS) ct_emf_col_kernel(
 
 // face update by the discrete curl of the edge EMFs, plain or Kahan (ct.jl:96-129)
 template <bool COMP>
-static __global__ void __launch_bounds__(AUX_THREADS) ct_face_col_kernel(
-    const float* __restrict__ ex, const float* __restrict__ ey, const float* __restrict__ ez,
-    float* __restrict__ bxf, float* __restrict__ byf, float* __restrict__ bzf, float* __restrict__ rbx,
-    float* __restrict__ rby, float* __restrict__ rbz, int nx, int ny, int nz, float dtdx) {
-  const int i = blockIdx.x * CTC_X + (threadIdx.x & 31), j = blockIdx.y * CTC_Y + (threadIdx.x >> 5);
+__device__ __forceinline__ void ct_face_col(const float* __restrict__ ex, const float* __restrict__ ey,
+                                            const float* __restrict__ ez, float* __restrict__ bxf,
+                                            float* __restrict__ byf, float* __restrict__ bzf, float* __restrict__ rbx,
+                                            float* __restrict__ rby, float* __restrict__ rbz, int nx, int ny, int nz,
+                                            float dtdx, int tx, int ty, int tz) {
+  const int i = tx * CTC_X + (threadIdx.x & 31), j = ty * CTC_Y + (threadIdx.x >> 5);
   if (i >= nx || j >= ny) return;
-  const int z0 = blockIdx.z * CTC_Z, z1 = min(z0 + CTC_Z, nz);
+  const int z0 = tz * CTC_Z, z1 = min(z0 + CTC_Z, nz);
   const size_t nxy = (size_t)nx * ny;
   const size_t o = (size_t)j * nx + i, oip = (size_t)j * nx + wrap_inc(i, nx), ojp = (size_t)wrap_inc(j, ny) * nx + i;
   // plane k values that plane k-1 read as its upper neighbour
@@ -318,34 +233,58 @@ static __global__ void __launch_bounds__(AUX_THREADS) ct_face_col_kernel(
   }
 }
 
-// cell B = face average (ct.jl:132-143) and the new state's signal speed
+// cell B = face average (ct.jl:132-143); returns this thread's max signal speed of the new
+// state (0 without want_speed). Every thread returns: the caller reduces over the block.
+__device__ __forceinline__ float ct_bcc_col(const float* __restrict__ bxf, const float* __restrict__ byf,
+                                            const float* __restrict__ bzf, const MPtr9& Un, int nx, int ny, int nz,
+                                            const Phys& P, bool want_speed, int tx, int ty, int tz) {
+  const int i = tx * CTC_X + (threadIdx.x & 31), j = ty * CTC_Y + (threadIdx.x >> 5);
+  float m = 0.0f;
+  if (i >= nx || j >= ny) return m;
+  const int z0 = tz * CTC_Z, z1 = min(z0 + CTC_Z, nz);
+  const size_t nxy = (size_t)nx * ny;
+  const size_t o = (size_t)j * nx + i, oip = (size_t)j * nx + wrap_inc(i, nx), ojp = (size_t)wrap_inc(j, ny) * nx + i;
+  float bz_c = bzf[(size_t)z0 * nxy + o];
+  for (int k = z0; k < z1; ++k) {
+    const size_t b = (size_t)k * nxy, c = b + o;
+    const float bz_kp = bzf[(size_t)wrap_inc(k, nz) * nxy + o];
+    const float bx = 0.5f * (bxf[c] + bxf[b + oip]);
+    const float by = 0.5f * (byf[c] + byf[b + ojp]);
+    const float bz = 0.5f * (bz_c + bz_kp);
+    F9 u{{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, bx, by, bz, 0.0f}};
+    if (want_speed)
+      for (int f = 0; f < 5; ++f) u[f] = Un.p[f][c];
+    Un.p[5][c] = bx;
+    Un.p[6][c] = by;
+    Un.p[7][c] = bz;
+    if (want_speed) m = fmaxf(m, cell_wavespeed(u, P));
+    bz_c = bz_kp;
+  }
+  return m;
+}
+
+static __global__ void __launch_bounds__(AUX_THREADS) ct_emf_col_kernel(
+    const float* __restrict__ MFX, const float* __restrict__ MFY, const float* __restrict__ MFZ,
+    const float* __restrict__ FXBY, const float* __restrict__ FXBZ, const float* __restrict__ FYBX,
+    const float* __restrict__ FYBZ, const float* __restrict__ FZBX, const float* __restrict__ FZBY,
+    const float* __restrict__ ECX, const float* __restrict__ ECY, const float* __restrict__ ECZ,
+    float* __restrict__ EX, float* __restrict__ EY, float* __restrict__ EZ, int nx, int ny, int nz) {
+  ct_emf_col(MFX, MFY, MFZ, FXBY, FXBZ, FYBX, FYBZ, FZBX, FZBY, ECX, ECY, ECZ, EX, EY, EZ, nx, ny, nz, blockIdx.x,
+             blockIdx.y, blockIdx.z);
+}
+
+template <bool COMP>
+static __global__ void __launch_bounds__(AUX_THREADS) ct_face_col_kernel(
+    const float* __restrict__ ex, const float* __restrict__ ey, const float* __restrict__ ez,
+    float* __restrict__ bxf, float* __restrict__ byf, float* __restrict__ bzf, float* __restrict__ rbx,
+    float* __restrict__ rby, float* __restrict__ rbz, int nx, int ny, int nz, float dtdx) {
+  ct_face_col<COMP>(ex, ey, ez, bxf, byf, bzf, rbx, rby, rbz, nx, ny, nz, dtdx, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 static __global__ void __launch_bounds__(AUX_THREADS) ct_bcc_col_kernel(
     const float* __restrict__ bxf, const float* __restrict__ byf, const float* __restrict__ bzf, const MPtr9 Un,
     int nx, int ny, int nz, Phys P, unsigned int* smax_bits) {
-  const int i = blockIdx.x * CTC_X + (threadIdx.x & 31), j = blockIdx.y * CTC_Y + (threadIdx.x >> 5);
-  float m = 0.0f;
-  if (i < nx && j < ny) {  // no early return: every thread joins the block reduction
-    const int z0 = blockIdx.z * CTC_Z, z1 = min(z0 + CTC_Z, nz);
-    const size_t nxy = (size_t)nx * ny;
-    const size_t o = (size_t)j * nx + i, oip = (size_t)j * nx + wrap_inc(i, nx),
-                 ojp = (size_t)wrap_inc(j, ny) * nx + i;
-    float bz_c = bzf[(size_t)z0 * nxy + o];
-    for (int k = z0; k < z1; ++k) {
-      const size_t b = (size_t)k * nxy, c = b + o;
-      const float bz_kp = bzf[(size_t)wrap_inc(k, nz) * nxy + o];
-      const float bx = 0.5f * (bxf[c] + bxf[b + oip]);
-      const float by = 0.5f * (byf[c] + byf[b + ojp]);
-      const float bz = 0.5f * (bz_c + bz_kp);
-      F9 u{{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, bx, by, bz, 0.0f}};
-      if (smax_bits != nullptr)
-        for (int f = 0; f < 5; ++f) u[f] = Un.p[f][c];
-      Un.p[5][c] = bx;
-      Un.p[6][c] = by;
-      Un.p[7][c] = bz;
-      if (smax_bits != nullptr) m = fmaxf(m, cell_wavespeed(u, P));
-      bz_c = bz_kp;
-    }
-  }
+  float m = ct_bcc_col(bxf, byf, bzf, Un, nx, ny, nz, P, smax_bits != nullptr, blockIdx.x, blockIdx.y, blockIdx.z);
   if (smax_bits != nullptr) {
     m = block_reduce_max(m);
     if (threadIdx.x == 0) atomicMax(smax_bits, __float_as_uint(m));

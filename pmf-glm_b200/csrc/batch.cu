@@ -6,8 +6,9 @@
 //      splits the concatenated (column, plane) spaces of its boxes evenly over the CTAs;
 //      each box reads its own {dt/dx, ch, decay} from device memory and reduces the max
 //      signal speed of its new state into its own slot;
-//   2. for constrained-transport boxes, the EMF / face / cell-B kernels over all CT boxes
-//      (blocks assigned per box, so each block reduces one box's signal speed);
+//   2. for constrained-transport boxes, the EMF / face / cell-B column kernels over all CT
+//      boxes (each block one 32 x 8 x 16 column tile of one box, so each block reduces one
+//      box's signal speed);
 //   3. one thread per box turns its signal speed into the next step's dt, ch and decay the
 //      way `evolve!` does (driver.jl:48-71, timestep.jl:37-41) and advances its clock.
 // Nothing returns to the host between steps.
@@ -27,8 +28,6 @@ using namespace pmf;
 using namespace pmf::host;
 
 namespace {
-
-constexpr int kCellsPerBlock = AUX_THREADS * 8;
 
 struct BoxMeta {
   float cfl, ch_fac, cr, dx;
@@ -57,32 +56,51 @@ __device__ __forceinline__ int find_view(const CtView* v, int n, int blk) {
   return lo;
 }
 
+// The block's column tile of its box: blocks block0.. of a box enumerate its (tx, ty, tz)
+// tiles of the column kernels, x fastest.
+__device__ __forceinline__ void col_tile(const CtView& b, int blk, int& tx, int& ty, int& tz) {
+  const int ntx = (b.nx + CTC_X - 1) / CTC_X, nty = (b.ny + CTC_Y - 1) / CTC_Y;
+  const int l = blk - b.block0;
+  tx = l % ntx;
+  ty = (l / ntx) % nty;
+  tz = l / (ntx * nty);
+}
+
+__device__ __forceinline__ float* ct_slot(const CtView& b, int k) {
+  return b.ct + (size_t)k * ((size_t)b.nx * b.ny * b.nz);
+}
+
 __global__ void __launch_bounds__(AUX_THREADS) batch_ct_emf_kernel(const CtView* __restrict__ v, int n) {
   const CtView& b = v[find_view(v, n, blockIdx.x)];
-  const int nc = b.nx * b.ny * b.nz;
-  const int base = (blockIdx.x - b.block0) * kCellsPerBlock;
-  for (int c = base + threadIdx.x; c < min(nc, base + kCellsPerBlock); c += AUX_THREADS)
-    ct_emf_cell(b.ct, b.nx, b.ny, b.nz, c);
+  int tx, ty, tz;
+  col_tile(b, blockIdx.x, tx, ty, tz);
+  ct_emf_col(ct_slot(b, CT_MFX), ct_slot(b, CT_MFY), ct_slot(b, CT_MFZ), ct_slot(b, CT_FXBY), ct_slot(b, CT_FXBZ),
+             ct_slot(b, CT_FYBX), ct_slot(b, CT_FYBZ), ct_slot(b, CT_FZBX), ct_slot(b, CT_FZBY), ct_slot(b, CT_ECX),
+             ct_slot(b, CT_ECY), ct_slot(b, CT_ECZ), ct_slot(b, CT_EX), ct_slot(b, CT_EY), ct_slot(b, CT_EZ), b.nx,
+             b.ny, b.nz, tx, ty, tz);
 }
 
 __global__ void __launch_bounds__(AUX_THREADS) batch_ct_face_kernel(const CtView* __restrict__ v, int n) {
   const CtView& b = v[find_view(v, n, blockIdx.x)];
-  const int nc = b.nx * b.ny * b.nz;
-  const int base = (blockIdx.x - b.block0) * kCellsPerBlock;
+  int tx, ty, tz;
+  col_tile(b, blockIdx.x, tx, ty, tz);
   const float dtdx = b.dscal[0];
-  for (int c = base + threadIdx.x; c < min(nc, base + kCellsPerBlock); c += AUX_THREADS) {
-    if (b.comp_faces) ct_face_cell<true>(b.ct, b.nx, b.ny, b.nz, dtdx, c);
-    else ct_face_cell<false>(b.ct, b.nx, b.ny, b.nz, dtdx, c);
-  }
+  if (b.comp_faces)
+    ct_face_col<true>(ct_slot(b, CT_EX), ct_slot(b, CT_EY), ct_slot(b, CT_EZ), ct_slot(b, CT_BXF), ct_slot(b, CT_BYF),
+                      ct_slot(b, CT_BZF), ct_slot(b, CT_RBX), ct_slot(b, CT_RBY), ct_slot(b, CT_RBZ), b.nx, b.ny,
+                      b.nz, dtdx, tx, ty, tz);
+  else
+    ct_face_col<false>(ct_slot(b, CT_EX), ct_slot(b, CT_EY), ct_slot(b, CT_EZ), ct_slot(b, CT_BXF),
+                       ct_slot(b, CT_BYF), ct_slot(b, CT_BZF), ct_slot(b, CT_RBX), ct_slot(b, CT_RBY),
+                       ct_slot(b, CT_RBZ), b.nx, b.ny, b.nz, dtdx, tx, ty, tz);
 }
 
 __global__ void __launch_bounds__(AUX_THREADS) batch_ct_bcc_kernel(const CtView* __restrict__ v, int n) {
   const CtView& b = v[find_view(v, n, blockIdx.x)];
-  const int nc = b.nx * b.ny * b.nz;
-  const int base = (blockIdx.x - b.block0) * kCellsPerBlock;
-  float m = 0.0f;
-  for (int c = base + threadIdx.x; c < min(nc, base + kCellsPerBlock); c += AUX_THREADS)
-    m = fmaxf(m, ct_bcc_cell(b.ct, b.Un, b.nx, b.ny, b.nz, b.P, true, c));
+  int tx, ty, tz;
+  col_tile(b, blockIdx.x, tx, ty, tz);
+  float m = ct_bcc_col(ct_slot(b, CT_BXF), ct_slot(b, CT_BYF), ct_slot(b, CT_BZF), b.Un, b.nx, b.ny, b.nz, b.P, true,
+                       tx, ty, tz);
   m = block_reduce_max(m);
   if (threadIdx.x == 0) atomicMax(b.smax_bits, __float_as_uint(m));
 }
@@ -295,7 +313,6 @@ int pmfmhd_batch_create(pmfmhd_ctx* c, const pmfmhd_box* boxes, int nbox, pmfmhd
   for (int i = 0; i < nbox; ++i) {
     const pmfmhd_box& x = boxes[i];
     if (x.mhd_solver != 1) continue;
-    const long long nc = ncells(&x.grid);
     for (int p = 0; p < 2; ++p) {
       CtView v;
       v.ct = x.ct_packed;
@@ -308,7 +325,8 @@ int pmfmhd_batch_create(pmfmhd_ctx* c, const pmfmhd_box* boxes, int nbox, pmfmhd
       v.comp_faces = x.resid[0] != nullptr;
       views[p].push_back(v);
     }
-    blk += (int)((nc + kCellsPerBlock - 1) / kCellsPerBlock);
+    const dim3 tiles = ctc_grid(x.grid.nx, x.grid.ny, x.grid.nz);  // column tiles of this box
+    blk += (int)(tiles.x * tiles.y * tiles.z);
   }
   b->nct = (int)views[0].size();
   b->ct_blocks = blk;
