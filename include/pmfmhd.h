@@ -137,7 +137,7 @@ int pmfmhd_step_ct_drag(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* cons
 #define PMFMHD_RAD_TRACK_ENERGY 4          /* Kahan-compensate E and the drag work (slot 8) */
 #define PMFMHD_RAD_CHECK_ADMISSIBILITY 8   /* write -max(|rho|, max(smallr, llf_dmin)) for rejected cells */
 #define PMFMHD_RAD_ROBUST_FALLBACK 16      /* minmod PLM with HLL on every face */
-#define PMFMHD_RAD_GLOBAL_FALLBACK 32      /* LLF on every face, with the admissibility check */
+#define PMFMHD_RAD_GLOBAL_FALLBACK 32      /* piecewise-constant states and LLF on every face, with the admissibility check */
 /*
  * Radiation-coupled step: the drag step (target at rest, impulse drag_impulse) whose face
  * states also carry a per-cell velocity correction, with optional tracking of the density

@@ -262,13 +262,21 @@ template <class T> Q<T> loadP(const Grid& g, const T* U, long nc, int i, int j, 
 }
 
 // integrator_ref.jl:17-26 — a cell's Hancock-predicted primitive and its per-axis offsets.
+// first_order: zero offsets, the piecewise-constant states of the cube kernel's global
+// fallback (CHECK == 3, integrator_cube.jl:168-177).
 template <class T> struct Edges { Q<T> m0, mh, dL[3], dR[3]; };
-template <class T> Edges<T> mh_edges(const Grid& g, const T* U, long nc, int i, int j, int k, T dtdx, const Phys<T>& P) {
+template <class T> Edges<T> mh_edges(const Grid& g, const T* U, long nc, int i, int j, int k, T dtdx, const Phys<T>& P,
+                                     bool first_order = false) {
   Edges<T> e;
   e.m0 = loadP(g, U, nc, i, j, k, P);
-  recon_offsets(loadP(g, U, nc, i - 1, j, k, P), e.m0, loadP(g, U, nc, i + 1, j, k, P), P.recon, e.dL[0], e.dR[0]);
-  recon_offsets(loadP(g, U, nc, i, j - 1, k, P), e.m0, loadP(g, U, nc, i, j + 1, k, P), P.recon, e.dL[1], e.dR[1]);
-  recon_offsets(loadP(g, U, nc, i, j, k - 1, P), e.m0, loadP(g, U, nc, i, j, k + 1, P), P.recon, e.dL[2], e.dR[2]);
+  if (first_order) {
+    for (int d = 0; d < 3; ++d)
+      for (int v = 0; v < 9; ++v) e.dL[d][v] = e.dR[d][v] = T(0);
+  } else {
+    recon_offsets(loadP(g, U, nc, i - 1, j, k, P), e.m0, loadP(g, U, nc, i + 1, j, k, P), P.recon, e.dL[0], e.dR[0]);
+    recon_offsets(loadP(g, U, nc, i, j - 1, k, P), e.m0, loadP(g, U, nc, i, j + 1, k, P), P.recon, e.dL[1], e.dR[1]);
+    recon_offsets(loadP(g, U, nc, i, j, k - 1, P), e.m0, loadP(g, U, nc, i, j, k + 1, P), P.recon, e.dL[2], e.dR[2]);
+  }
   Q<T> uh = hancock_edges(e.m0, e.dL, e.dR, dtdx, P.gamma);
   e.mh = cons2prim(uh, P.gamma, P.smallr, P.pfl);
   return e;
@@ -350,7 +358,7 @@ template <class T> Q<T> drag_correct_conserved(const Q<T>& u0, const Q<T>& trial
 // the velocity corrections added to every face state, slot 4 the accumulated density
 // increment (track_density), slots 5-7 the Kahan remainders of cell B (track_magnetic,
 // GLM only) and slot 8 that of E (track_energy).
-enum { RAD_TRACK_DENSITY = 1, RAD_TRACK_MAGNETIC = 2, RAD_TRACK_ENERGY = 4, RAD_CHECK = 8 };
+enum { RAD_TRACK_DENSITY = 1, RAD_TRACK_MAGNETIC = 2, RAD_TRACK_ENERGY = 4, RAD_CHECK = 8, RAD_FIRST_ORDER = 16 };
 template <class T> struct Rad {
   T* corr;   // null: no radiation coupling
   int flags;
@@ -382,12 +390,13 @@ void godunov(const Grid& g, const T* U, T* Un, T dtdx, T ch, T decay, const Phys
 #pragma omp parallel for schedule(dynamic, 64)
   for (long c = 0; c < nc; ++c) {
     int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long)g.nx * g.ny));
-    Edges<T> ec = mh_edges(g, U, nc, i, j, k, dtdx, P);
+    const bool fo = rad.corr != nullptr && (rad.flags & RAD_FIRST_ORDER) != 0;
+    Edges<T> ec = mh_edges(g, U, nc, i, j, k, dtdx, P, fo);
     Q<T> Fl[3], Fh[3];
     const int off[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
     for (int d = 0; d < 3; ++d) {
-      Edges<T> em = mh_edges(g, U, nc, i - off[d][0], j - off[d][1], k - off[d][2], dtdx, P);
-      Edges<T> ep = mh_edges(g, U, nc, i + off[d][0], j + off[d][1], k + off[d][2], dtdx, P);
+      Edges<T> em = mh_edges(g, U, nc, i - off[d][0], j - off[d][1], k - off[d][2], dtdx, P, fo);
+      Edges<T> ep = mh_edges(g, U, nc, i + off[d][0], j + off[d][1], k + off[d][2], dtdx, P, fo);
       // face states mh + offset, drag-propagated when drag is on, plus the radiation velocity
       // correction of the owning cell (integrator_ref.jl:28-39)
       auto face = [&](const Edges<T>& e, const Q<T>& off, long cell) {

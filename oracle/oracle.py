@@ -134,7 +134,7 @@ class OracleState:
                                      float(T(ch)), float(decay), float(T(drag_impulse)), v0)
         self.U, self.scratch = self.scratch, self.U
 
-    RAD_TRACK_DENSITY, RAD_TRACK_MAGNETIC, RAD_TRACK_ENERGY, RAD_CHECK = 1, 2, 4, 8
+    RAD_TRACK_DENSITY, RAD_TRACK_MAGNETIC, RAD_TRACK_ENERGY, RAD_CHECK, RAD_FIRST_ORDER = 1, 2, 4, 8, 16
 
     def step_radiation(self, dt, drag_impulse, correction, ch=0.0, decay=1.0, track_density=True,
                        track_magnetic=True, track_energy=True, check_admissibility=False, robust_fallback=False,
@@ -142,14 +142,16 @@ class OracleState:
         """The radiation-coupled step kernel: step_ref_radiation! (integrator_ref.jl:238-258) and
         step_cube_radiation! (integrator_cube.jl:504-540). ``correction`` is the packed (9, nc)
         buffer of the state precision; its slot 0 is read as psi, slots 4-8 are updated.
-        robust_fallback: minmod PLM with HLL; global_fallback: LLF on every face (with the
-        admissibility flag)."""
+        robust_fallback: minmod PLM with HLL; global_fallback: piecewise-constant states and LLF
+        on every face, with the admissibility flag (CHECK == 3, integrator_cube.jl:168-177,
+        524-529)."""
         T = self.T
         corr = correction
         assert corr.dtype == self.U.dtype and corr.shape == (9, self.nc) and corr.flags["C_CONTIGUOUS"]
         flags = ((self.RAD_TRACK_DENSITY if track_density else 0) | (self.RAD_TRACK_MAGNETIC if track_magnetic else 0)
                  | (self.RAD_TRACK_ENERGY if track_energy else 0)
-                 | (self.RAD_CHECK if (check_admissibility or global_fallback) else 0))
+                 | (self.RAD_CHECK if (check_admissibility or global_fallback) else 0)
+                 | (self.RAD_FIRST_ORDER if global_fallback else 0))
         saved = (self.p.recon, self.p.riemann)
         if robust_fallback:
             self.p.recon, self.p.riemann = RECON["plm_minmod"], RIEMANN["hll"]

@@ -526,8 +526,10 @@ int pmfmhd_step_radiation(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* cons
     g2.riemann = PMFMHD_RIEMANN_HLL;
   } else if (flags & PMFMHD_RAD_GLOBAL_FALLBACK) {
     g2.riemann = PMFMHD_RIEMANN_LLF;
-    rf |= RAD_CHECK;
   }
+  // integrator_cube.jl:524-529: the global fallback launches with CHECK == 3, piecewise-constant
+  // states and the admissibility test (with the robust solver if both are asked for)
+  if (flags & PMFMHD_RAD_GLOBAL_FALLBACK) rf |= RAD_CHECK | RAD_FIRST_ORDER;
   // psi is read from slot 0 of the correction buffer, as the reference passes the buffer in
   // place of U[9]
   const float* Uin[9];

@@ -152,6 +152,15 @@ template <> struct Offsets<RECON_PPM> {
   __device__ __forceinline__ float l(int i) const { return dL[i]; }
 };
 
+// Offsets times k (k = 0: the piecewise-constant states of a first-order fallback).
+template <int RECON> __device__ __forceinline__ void scale_offsets(Offsets<RECON>& o, float k) {
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    o.dR[i] *= k;
+    if constexpr (RECON == RECON_PPM) o.dL[i] *= k;
+  }
+}
+
 // Half the MonCen slope, 0.5*moncen(dl, dr) of glm_physics.jl:47-53, with the scalings by
 // powers of two folded: 0.5*sgn*min(2*min|dl|,|dr|, |(dl+dr)/2|) = sgn*min(min(|dl|,|dr|),
 // |dl+dr|/4). Every rescaling is exact, so the result has the same bits.

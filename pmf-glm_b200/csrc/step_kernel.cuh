@@ -74,7 +74,9 @@ struct StepArgs {
 // Source terms of the step (template parameter SRC of the step kernel).
 enum { SRC_NONE = 0, SRC_DRAG = 1, SRC_RAD = 2 };
 // Runtime options of the radiation-coupled step (StepArgs::rad_flags).
-enum { RAD_TRACK_DENSITY = 1, RAD_TRACK_MAGNETIC = 2, RAD_TRACK_ENERGY = 4, RAD_CHECK = 8 };
+// RAD_FIRST_ORDER: zero reconstruction offsets in every cell, the piecewise-constant states of
+// the cube kernel's global fallback (CHECK == 3, integrator_cube.jl:168-177).
+enum { RAD_TRACK_DENSITY = 1, RAD_TRACK_MAGNETIC = 2, RAD_TRACK_ENERGY = 4, RAD_CHECK = 8, RAD_FIRST_ORDER = 16 };
 
 template <int TY>
 struct StepSmem {
@@ -430,6 +432,14 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     ox = recon<RECON>(ld9(p0, r0, c0 - 1), m0, ld9(p0, r0, c0 + 1));
     oy = recon<RECON>(ld9(p0, r0 - 1, c0), m0, ld9(p0, r0 + 1, c0));
     oz = recon<RECON>(ld9(pm, r0, c0), m0, ld9(pp, r0, c0));
+    if constexpr (RAD) {
+      // piecewise-constant states: offsets scaled by 0 (m0 + (+-0) == m0, so every face state
+      // and Hancock flux difference is that of zero offsets), without a branch
+      const float keep = (a.rad_flags & RAD_FIRST_ORDER) ? 0.0f : 1.0f;
+      scale_offsets(ox, keep);
+      scale_offsets(oy, keep);
+      scale_offsets(oz, keep);
+    }
     {
       const F9 u0 = prim2cons(m0, g);
       F9 acc = hancock_term<0, RECON>(m0, ox, g);

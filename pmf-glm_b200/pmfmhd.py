@@ -437,8 +437,9 @@ def step_cube_radiation(s: MHDState, dt: float, ch: float, decay: float, drag_im
                         check_admissibility: bool = False, fallback: bool = False, global_fallback: bool = False,
                         robust_fallback: bool = False) -> MHDState:
     """integrator_cube.jl:504-540 (GLM states): as step_ref_radiation, plus the admissibility
-    flag (rejected cells get density -max(|rho|, max(smallr, llf_dmin))) and the global LLF
-    fallback. The masked per-face fallback (``fallback=True``) is not provided."""
+    flag (rejected cells get density -max(|rho|, max(smallr, llf_dmin))) and the global
+    fallback (piecewise-constant states with LLF, the cube kernel's CHECK == 3). The masked
+    per-face fallback (``fallback=True``) is not provided."""
     if uses_ct(s):
         raise PMFMHDError("step_cube_radiation!: CT is implemented on the :ref integrator only "
                           "(mhd_solver=:ct states cannot use the :cube integrators)")

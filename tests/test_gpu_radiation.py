@@ -151,6 +151,23 @@ def test_admissibility_flag_and_fallbacks_match_oracle(mode):
     corr_parity(corr_d.cpu().numpy().reshape(9, -1), corr_h)
 
 
+def test_global_fallback_is_first_order_on_device():
+    """The global fallback zeroes every reconstruction offset (CHECK == 3,
+    integrator_cube.jl:168-177): PLM and PPM states step to the same result (to FP32 rounding:
+    the two instantiations may contract multiply-adds differently)."""
+    dims = (24, 12, 10)
+    U = problems.turb_field(dims, 1.0 / 24)
+    nc = int(np.prod(dims))
+    outs = []
+    for recon in ("plm", "ppm"):
+        dev = gpu_state(U, dims, recon=recon)
+        corr = torch.from_numpy(corrections(nc, 5, U[8], scale=0.0).ravel().copy()).cuda()
+        pmfmhd.step_cube_radiation(dev, 2e-3, 1.0, 1.0, 0.1, corr, global_fallback=True)
+        outs.append(pmfmhd.fields_to_host(dev).astype(np.float64))
+    for f in range(8):
+        assert np.abs(outs[1][f] - outs[0][f]).max() <= 1e-6 * np.abs(outs[0][f]).max()
+
+
 def test_radiation_argument_errors():
     n = 8
     s = gpu_state(problems.smooth_fields(n), (n, n, n))
