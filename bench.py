@@ -41,7 +41,39 @@ def parse():
                     help="time only the constrained-transport step of the --n box (for kernel profiling)")
     ap.add_argument("--drag-only", action="store_true",
                     help="time only the drag-coupled GLM step (SRC_DRAG) of the --n box")
+    ap.add_argument("--compensated-only", action="store_true",
+                    help="time only the compensated GLM step of the --n box (for kernel profiling)")
     return ap.parse_args()
+
+
+def compensated_only(args):
+    """The compensated GLM step (Kahan remainders of momentum, E and B) on the headline box:
+    one JSON line with its device time per step."""
+    import torch
+
+    import ics
+    import pmfmhd
+    n = args.n
+    s = pmfmhd.set_fields(pmfmhd.allocate_state((n, n, n), 1.0 / n, compensated=True),
+                          ics.turbulent_box(n, seed=0)["U"])
+    dt, sp = pmfmhd.compute_dt(s, 0.2)
+    decay = float(np.exp(np.float32(np.float32(np.float32(-0.18) * np.float32(sp)) * np.float32(dt)) / np.float32(s.dx)))
+    pmfmhd.autotune(s)
+    for _ in range(args.warmup):
+        pmfmhd.step_cube(s, dt, sp, decay)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(args.steps):
+        pmfmhd.step_cube(s, dt, sp, decay)
+    a1.record(stream)
+    torch.cuda.synchronize()
+    ms = a0.elapsed_time(a1) / args.steps
+    host = pmfmhd.fields_to_host(s)
+    print(json.dumps({"compensated_only": True, "n": n, "steps": args.steps, "ms_per_step": ms,
+                      "value": n ** 3 / (ms / 1e3), "unit": UNIT, "tile": list(pmfmhd.get_tile(s)),
+                      "finite": bool(np.isfinite(host).all())}))
 
 
 def drag_only(args):
@@ -490,6 +522,9 @@ def main():
         return
     if args.drag_only:
         drag_only(args)
+        return
+    if args.compensated_only:
+        compensated_only(args)
         return
     import torch
     import torch.distributed as dist
