@@ -150,6 +150,26 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def issue_roof(n, kernel_ms, clocks, device):
+    """The FP32-issue side of the roofline: warp instructions per cell of the step kernel (from
+    the committed ncu capture) x cells / kernel time, against what the SMs can issue at the
+    sampled median SM clock (one warp instruction per sub-partition per cycle, 4 per SM)."""
+    import torch
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(tf):
+        return None
+    t = json.load(open(tf))
+    wi = t.get("glm_warp_inst_per_cell")
+    mhz = (clocks or {}).get("sm_mhz")
+    if wi is None or not mhz:
+        return None
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    achieved = float(wi) * n ** 3 / (kernel_ms / 1e3)
+    peak = sms * 4 * float(mhz) * 1e6
+    return {"bound": "fp32_issue", "achieved": achieved, "peak": peak, "unit": "warp-instructions/s",
+            "frac": achieved / peak, "warp_inst_per_cell": float(wi), "sm_mhz": float(mhz), "sms": sms}
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle samples while the GPU is busy."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -187,60 +207,94 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows), "samples_under_load": len(load)}
 
 
-def cpu_baseline(n=64, steps=6):
-    """The oracle (C++ restatement of the reference's per-cell :ref scheme), FP32, all host
-    threads, on an n^3 box of the same generator: a bounded sample of the workload."""
-    import ics
+def host_cores():
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+
+
+def _oracle_rate(U, n, steps):
+    """Zone-updates/s of the oracle FP32 :ref scheme on the n^3 state U (one untimed step,
+    then `steps` timed ones)."""
     import oracle
-    box = ics.turbulent_box(n, seed=0)
     s = oracle.OracleState((n, n, n), 1 / n, dtype=np.float32)
-    s.U[:] = box["U"]
+    s.U[:] = U
     dt, sp = s.compute_dt(0.2)
-    s.step(dt, ch=sp)  # warm
+    s.step(dt, ch=sp)
     t0 = time.perf_counter()
     for _ in range(steps):
         s.step(dt, ch=sp)
     el = time.perf_counter() - t0
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": n ** 3 * steps / el, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"oracle FP32 :ref scheme, {n}^3 box of the same generator, {steps} steps, {el:.1f} s"}
+    return n ** 3 * steps / el, el
+
+
+def cpu_baseline(U256):
+    """The oracle (C++ restatement of the reference's per-cell :ref scheme, the reference's CPU
+    default integrator), FP32, all host threads, on 64^3, 128^3 and the headline 256^3 box of
+    the same generator: bounded samples of the workload; `value` is the 256^3 row."""
+    import ics
+    rows = []
+    for n, steps in ((64, 6), (128, 2)):
+        v, el = _oracle_rate(ics.turbulent_box(n, seed=0)["U"], n, steps)
+        rows.append({"n": n, "steps": steps, "seconds": round(el, 2), "value": v})
+    v, el = _oracle_rate(U256, 256, 1)
+    rows.append({"n": 256, "steps": 1, "seconds": round(el, 2), "value": v})
+    return {"value": v, "unit": UNIT, "cores": host_cores(), "kind": "port",
+            "sample": f"oracle FP32 :ref scheme on the 256^3 headline box, 1 step ({el:.1f} s) after one untimed "
+                      "step; rows: 64^3, 128^3, 256^3 of the same generator",
+            "rows": rows}
+
+
+REFERENCE_BUDGET_S = 150.0  # wall time the reference arm may spend in warm-up and timed steps
 
 
 def run_reference(args):
+    """The reference arm: the reference's CPU scheme (the oracle's FP32 restatement of the
+    per-cell :ref integrator; the reference is Julia, which this image cannot run) on the
+    headline box, all host threads. Each step is a full step of the --n box when warm-up and
+    timed steps fit REFERENCE_BUDGET_S at the rate of a first probe step; otherwise each step
+    is a bounded sample, the same z-slab of that box every step (zone-updates counted over the
+    slab). Under torchrun only rank 0 runs."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     import ics
     import oracle
-    n = 64
-    box = ics.turbulent_box(n, seed=0)
+    n = args.n
     s = oracle.OracleState((n, n, n), 1 / n, dtype=np.float32)
-    s.U[:] = box["U"]
+    s.U[:] = ics.turbulent_box(n, seed=0)["U"]
     dt, sp = s.compute_dt(0.2)
+    t0 = time.perf_counter()
+    s.step_planes(dt, sp, 0, max(1, n // 16))  # probe: the rate of the scheme on this box
+    probe = (time.perf_counter() - t0) / max(1, n // 16) * n  # seconds per full step
+    total = args.steps + args.warmup
+    planes = n if probe * total <= REFERENCE_BUDGET_S else max(1, int(n * REFERENCE_BUDGET_S / (probe * total)))
+    z0 = (n - planes) // 2
     for _ in range(args.warmup):
-        s.step(dt, ch=sp)
+        s.step_planes(dt, sp, z0, z0 + planes)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        s.step(dt, ch=sp)
+        s.step_planes(dt, sp, z0, z0 + planes)
     el = time.perf_counter() - t0
-    value = n ** 3 * args.steps / el
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    value = n * n * planes * args.steps / el
+    sample = (f"each step: oracle FP32 :ref scheme (the reference's CPU integrator restated in C++; the reference "
+              f"is Julia and cannot run here) on the {n}^3 headline box, " +
+              ("the full box" if planes == n else f"a {planes}-plane z-slab of it (bounded sample)"))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(args.n, args.steps),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"each step: oracle FP32 :ref scheme on a {n}^3 box of the same generator "
-                                       "(the reference is Julia and cannot run here)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": host_cores(), "kind": "port", "sample": sample,
+                             "planes_per_step": planes},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def linf_vs_fp64(n=64, steps=20):
     """Config-0 accuracy: GPU FP32 (plain and compensated) against the FP64 oracle after
-    `steps` steps, per field relative to max|field| (L-inf, 99.9th percentile and mean), the
-    FP32 oracle (the reference scheme in FP32) beside it, and the energy-ledger drift.
-    HLL on the same box is the control without HLLD's near-degenerate star states."""
+    `steps` steps, per field relative to max|field| (L-inf, 99.9th percentile, mean and the
+    fraction of cells beyond 1e-5), the FP32 oracle (the reference scheme in FP32) beside it,
+    and the energy-ledger drift, in both HLLD degeneracy modes (each against the oracle of the
+    same mode), with the device census of near-degenerate HLLD sides over the run. HLL on the
+    same box is the control without HLLD's near-degenerate star states."""
     import ics
     import oracle
     import pmfmhd
@@ -252,28 +306,46 @@ def linf_vs_fp64(n=64, steps=20):
         return {"linf_rel_per_field": [float("%.3e" % x.max()) for x in d],
                 "linf_rel_max": float(max(x.max() for x in d)),
                 "p999_rel_max": float(max(np.quantile(x, 0.999) for x in d)),
-                "mean_rel_max": float(max(x.mean() for x in d))}
+                "mean_rel_max": float(max(x.mean() for x in d)),
+                "frac_beyond_1e-5_max": float(max((x > 1e-5).mean() for x in d))}
 
-    out = {"case": f"{n}^3 turbulent box, {steps} steps, CFL 0.2, MC-PLM; FP64 oracle as truth"}
-    for rs in ("hlld", "hll"):
-        ref = oracle.OracleState((n, n, n), 1 / n, dtype=np.float64, riemann=rs)
+    out = {"case": f"{n}^3 turbulent box, {steps} steps, CFL 0.2 fixed dt, MC-PLM; FP64 oracle of the same mode as truth"}
+    modes = {"relative": pmfmhd.HLLD_DTOL_RELATIVE, "reference": pmfmhd.HLLD_DTOL_REFERENCE}
+    truth = {}
+    for rs, mode in (("hlld", "relative"), ("hlld", "reference"), ("hll", "relative")):
+        tol = modes[mode]
+        ref = oracle.OracleState((n, n, n), 1 / n, dtype=np.float64, riemann=rs, hlld_dtol_rel=tol)
         ref.U[:] = U.astype(np.float64)
         dt, sp = ref.compute_dt(0.2)
         e0 = ref.conserved_totals()["energy"]
-        o32 = oracle.OracleState((n, n, n), 1 / n, dtype=np.float32, riemann=rs)
+        o32 = oracle.OracleState((n, n, n), 1 / n, dtype=np.float32, riemann=rs, hlld_dtol_rel=tol)
         o32.U[:] = U
         for _ in range(steps):
             ref.step(dt, ch=sp)
             o32.step(dt, ch=sp)
+        truth[(rs, mode)] = ref.U.copy()
         res = {"oracle_fp32": stats(o32.U, ref.U)}
         for comp in (False, True):
-            s = pmfmhd.set_fields(pmfmhd.allocate_state((n, n, n), 1 / n, riemann=rs, compensated=comp), U)
+            s = pmfmhd.set_fields(pmfmhd.allocate_state((n, n, n), 1 / n, riemann=rs, compensated=comp,
+                                                        hlld_dtol_rel=tol), U)
+            census = {"solves": 0, "ref_sides": 0, "rel_sides": 0}
             for _ in range(steps):
-                pmfmhd.step(s, float(dt), ch=float(sp))
+                if rs == "hlld" and not comp:
+                    T = np.float32
+                    decay = float(np.exp(T(T(-T(0.18) * T(sp) * T(dt)) / T(s.dx))))
+                    c = pmfmhd.step_census(s, float(dt), float(sp), decay)
+                    for k in census:
+                        census[k] += c[k]
+                else:
+                    pmfmhd.step(s, float(dt), ch=float(sp))
             r = stats(pmfmhd.fields_to_host(s), ref.U)
             r["energy_ledger_drift"] = abs(pmfmhd.conserved_totals(s)["energy"] - e0) / abs(e0)
+            if rs == "hlld" and not comp:
+                r["census"] = census
             res["compensated" if comp else "plain"] = r
-        out[rs] = res
+        out[rs if rs == "hll" else f"hlld_{mode}"] = res
+    a, b = truth[("hlld", "reference")], truth[("hlld", "relative")]
+    out["fp64_modes_linf_rel_max"] = float(max(np.abs(a[v] - b[v]).max() / np.abs(a[v]).max() for v in range(8)))
     return out
 
 
@@ -390,6 +462,53 @@ def big_box_cases():
     stress["accuracy_128"] = _accuracy_128(Ud, 40, "stress box averaged 4^3 -> 128^3")
     out["stress_512"] = stress
     return out
+
+
+def plain_port(s, U_host, dt, sp, decay, steps, warmup):
+    """The plain single-instance FP32 port (pmf-glm_b200/libpmfport.so: one thread per cell,
+    the reference's per-cell kernel with its seven Hancock predictions and six Riemann solves per
+    cell) on the same state and fixed dt: device ms per step."""
+    import ctypes
+
+    import torch
+
+    import pmfmhd
+    L = ctypes.CDLL(os.path.join(ROOT, "pmf-glm_b200", "libpmfport.so"))
+    L.pmfport_step_glm.argtypes = [ctypes.POINTER(pmfmhd.Grid), pmfmhd._P9, pmfmhd._P9, ctypes.c_float,
+                                   ctypes.c_float, ctypes.c_float, ctypes.c_void_p]
+    pmfmhd.set_fields(s, U_host)
+
+    def one():
+        rc = L.pmfport_step_glm(ctypes.byref(s.grid), pmfmhd._p9(s.U), pmfmhd._p9(s.scratch), float(dt), float(sp),
+                                float(decay), pmfmhd._stream())
+        if rc != 0:
+            raise RuntimeError(f"pmfport_step_glm: {rc}")
+        s.U, s.scratch = s.scratch, s.U
+    for _ in range(warmup):
+        one()
+    torch.cuda.synchronize()
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record()
+    for _ in range(steps):
+        one()
+    a1.record()
+    torch.cuda.synchronize()
+    return a0.elapsed_time(a1) / steps
+
+
+def census_run(s, U_host, dt, sp, decay, steps):
+    """HLLD census over `steps` fixed-dt steps of the state's grid from U_host."""
+    import pmfmhd
+    pmfmhd.set_fields(s, U_host)
+    tot = {"solves": 0, "ref_sides": 0, "rel_sides": 0}
+    per_step = []
+    for _ in range(steps):
+        c = pmfmhd.step_census(s, dt, sp, decay)
+        per_step.append(c["ref_sides"] + c["rel_sides"])
+        for k in tot:
+            tot[k] += c[k]
+    tot["near_degenerate_sides_per_step"] = per_step
+    return tot
 
 
 def build_boxes(specs):
@@ -580,7 +699,8 @@ def main():
     divb = pmfmhd.max_divb(s) * s.dx / brms
 
     extra = {"divb_centred_dx_over_brms": divb, "finite": bool(np.isfinite(host_after).all()),
-             "positive_density": bool(host_after[0].min() > 0), "kernel_ms": kernel_ms}
+             "positive_density": bool(host_after[0].min() > 0), "kernel_ms": kernel_ms,
+             "hlld_dtol_rel": pmfmhd.HLLD_DTOL_RELATIVE}
 
     # ---- end to end: host state in, host state out, through the C ABI, every step ----------
     # pmfmhd_step_glm_host: the state lives in pinned host memory; each call copies it in,
@@ -606,6 +726,34 @@ def main():
            "d2h_bytes_per_step": int(pin_out.numel() * 4)}
 
     if not args.quick:
+        # the same box with the reference's own HLLD degeneracy test (hlld_dtol_rel = 0): the
+        # same kernel, so the same speed; and the census of near-degenerate HLLD sides of the
+        # timed run in both modes (the faces where the modes differ)
+        r = pmfmhd.set_fields(pmfmhd.allocate_state((n, n, n), 1.0 / n, hlld_dtol_rel=pmfmhd.HLLD_DTOL_REFERENCE),
+                              U_host)
+        pmfmhd.autotune(r)
+        for _ in range(args.warmup):
+            pmfmhd.step_cube(r, dt, sp, decay)
+        pmfmhd.set_fields(r, U_host)
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(args.steps):
+            pmfmhd.step_cube(r, dt, sp, decay)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        rm = a0.elapsed_time(a1) / args.steps
+        hr = pmfmhd.fields_to_host(r)
+        extra["reference_mode"] = {"value": n ** 3 / (rm / 1e3), "ms_per_step": rm,
+                                   "finite": bool(np.isfinite(hr).all())}
+        extra["census"] = {"steps": args.steps,
+                           "relative": census_run(s, U_host, dt, sp, decay, args.steps),
+                           "reference": census_run(r, U_host, dt, sp, decay, args.steps)}
+        del r, hr
+        # the plain single-instance FP32 port of the reference's per-cell kernel, same box
+        port_ms = plain_port(s, U_host, dt, sp, decay, min(args.steps, 10), 2)
+        extra["plain_port"] = {"value": n ** 3 / (port_ms / 1e3), "ms_per_step": port_ms,
+                               "fused_speedup": port_ms / kernel_ms}
         # CT side by side on the same generator (faces from the edge potential)
         boxc = ics.turbulent_box(n, seed=0, with_ct=True)
         c = pmfmhd.set_fields(pmfmhd.allocate_state((n, n, n), 1.0 / n, mhd_solver="ct"), boxc["U"])
@@ -640,6 +788,7 @@ def main():
         torch.cuda.synchronize()
         cm = a0.elapsed_time(a1) / args.steps
         extra["compensated"] = {"value": n ** 3 / (cm / 1e3), "ms_per_step": cm}
+        extra["plain_port"]["compensated_speedup"] = extra["plain_port"]["ms_per_step"] / cm
         del q
         if world == 1:
             extra["batched"] = batched_mix()
@@ -663,13 +812,16 @@ def main():
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "peak_kind": peak_kind,
             "algorithmic_bytes_per_zone": BYTES_PER_ZONE_GLM}
+    issue = issue_roof(n, kernel_ms, clocks, local)
+    if issue is not None:
+        roof["issue"] = issue
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(n, args.steps),
             "roofline": roof, "e2e": e2e, "clocks": clocks, "gpu_launches": args.steps}
     if not args.quick and world == 1:
         line["accuracy"] = linf_vs_fp64()
-        line["cpu_baseline"] = cpu_baseline()
+        line["cpu_baseline"] = cpu_baseline(U_host)
     line["extra"] = extra
     print(json.dumps(line), flush=True)
     if world > 1:

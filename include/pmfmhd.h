@@ -44,13 +44,27 @@ extern "C" {
 #define PMFMHD_BC_OUTFLOW 1
 #define PMFMHD_BC_REFLECT 2
 
-/* Grid and run parameters: the scalar fields of MHDState (state.jl:63-79). */
+/* HLLD single-star degeneracy tolerances (pmfmhd_grid.hlld_dtol_rel). */
+#define PMFMHD_HLLD_DTOL_REFERENCE 0.0f /* the reference's test |denK| < 1e-12 */
+#define PMFMHD_HLLD_DTOL_RELATIVE 1e-5f /* |denK| < max(1e-12, 1e-5 bn^2) */
+
+/* Grid and run parameters: the scalar fields of MHDState (state.jl:63-79), plus the HLLD
+ * degeneracy tolerance. */
 typedef struct pmfmhd_grid {
   int32_t nx, ny, nz;
   int32_t bc[3];   /* per axis, PMFMHD_BC_* */
   int32_t recon;   /* PMFMHD_RECON_* */
   int32_t riemann; /* PMFMHD_RIEMANN_* */
   float dx, gamma, smallr, pfl, llf_dmin, llf_pmin;
+  /* HLLD single-star states (glm_physics.jl:255-263) fall back to the unmodified transverse
+   * state when |denK| < max(1e-12, hlld_dtol_rel * bn^2), denK = d(S-u)(S-SM) - bn^2.
+   * 0 (PMFMHD_HLLD_DTOL_REFERENCE) is the reference's own absolute test |denK| < 1e-12: the
+   * reference's arithmetic exactly. 1e-5 (PMFMHD_HLLD_DTOL_RELATIVE) widens it to the FP32
+   * rounding level of denK, where the single-star states are otherwise ~1/denK of rounding
+   * noise; it changes the flux only at those near-degenerate faces (a handful per step on a
+   * turbulent 256^3 box) and kept a 512^3 turbulent box finite that blew up with the absolute
+   * test. Must be finite and >= 0. */
+  float hlld_dtol_rel;
 } pmfmhd_grid;
 
 /* Opaque per-device context: reduction workspace, tile autotuning table, cached graphs. */
@@ -204,7 +218,10 @@ int pmfmhd_conserved_totals(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* 
  * GPU that loads it until exit. At most 2^24 cells (256^3); larger grids return
  * PMFMHD_ESHAPE. One partial sum per 256-cell block in a fixed order, so the result does not
  * depend on the SM count. Calls share the array: calls that overlap on the GPU race and
- * must be serialised. The first call on a device looks up the array's address; make it
+ * must be serialised. The first call in each CUDA context looks up the array's address and
+ * caches it with the context's id; a context re-created later (cudaDeviceReset, or a host that
+ * rebuilds its primary context) gets a fresh look-up on its first call, since the library's
+ * module, and with it the array, may then sit elsewhere. Make the first call of a context
  * before any stream capture. Blocking.
  */
 int pmfmhd_conserved_totals_noalloc(const pmfmhd_grid* g, const float* const U[9], double out[8], void* stream);
@@ -265,10 +282,34 @@ int pmfmhd_batch_destroy(pmfmhd_batch* b);
 int pmfmhd_autotune(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], int mhd_solver,
                     int compensated, void* stream);
 
+/*
+ * pmfmhd_step_glm (plain update, MC-PLM with HLLD only) that also counts the HLLD single-star
+ * degeneracy cases over every face of the grid once: out[0] = HLLD solves (faces not sent to
+ * the LLF fallback), out[1] = single-star sides with |denK| < 1e-12 (the reference's degenerate
+ * branch), out[2] = sides with 1e-12 <= |denK| < 1e-5 bn^2 (sent to the degenerate branch by
+ * the relative tolerance only, i.e. the faces where the two tolerances give different fluxes).
+ * The step is performed with g->hlld_dtol_rel as given. A diagnostic of the tolerance choice;
+ * no counterpart in the reference. PMFMHD_EUNSUPPORTED for other reconstructions or solvers.
+ * Blocking.
+ */
+int pmfmhd_step_glm_census(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],
+                           float dt, float ch, float decay, uint64_t out[3], void* stream);
+
+/*
+ * Test hook for the bounded TMA wait, normally 0. With polls > 0, every TMA-staged plane of
+ * the steps enqueued afterwards on this context arms its mbarrier without issuing the copies
+ * and gives up after `polls` polls: the wait runs out with nothing in flight, the status
+ * becomes PMFMHD_ETIMEOUT and the step finishes by loading its planes straight from global
+ * memory (its result is still the step's). polls = 0 restores normal staging.
+ */
+int pmfmhd_set_tma_stall(pmfmhd_ctx* ctx, int polls);
+
 /* Device status of the steps enqueued on this context since the last clearing call:
- * PMFMHD_ETIMEOUT if a step kernel's bounded wait for a TMA plane load gave up (that step's
- * result is invalid; staging fell back to per-element copies), else PMFMHD_OK. clear != 0
- * resets the status. Blocking. */
+ * PMFMHD_ETIMEOUT if a step kernel's bounded wait for a TMA plane load gave up, else
+ * PMFMHD_OK. After a give-up the launch stops using its staging buffer (a late copy may still
+ * land there) and loads every later plane straight from global memory, so the step still
+ * completes with its own result; before exiting, each CTA gives the outstanding copy one more
+ * bounded wait. clear != 0 resets the status. Blocking. */
 int pmfmhd_status(pmfmhd_ctx* ctx, int clear, void* stream);
 
 /* Pin (or query) the tile used for this grid/solver/mode on this context: `rows` owned rows

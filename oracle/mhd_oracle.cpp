@@ -41,6 +41,16 @@ template <class T> struct Q { T v[9]; T& operator[](int i) { return v[i]; } cons
 template <class T> struct Phys {
   T gamma, smallr, pfl, llf_dmin, llf_pmin;
   int recon, rsol;
+  // HLLD single-star degeneracy test |denK| < max(1e-12, dtol_rel * bn^2); dtol_rel = 0 is the
+  // reference's own test |denK| < 1e-12 (glm_physics.jl:257)
+  T dtol_rel;
+};
+
+// HLLD degeneracy census of one thread: solves, single-star sides with |denK| < 1e-12 (the
+// reference's degenerate branch) and sides with 1e-12 <= |denK| < 1e-5 bn^2 (sent to the
+// degenerate branch only by the relative test). Not part of the reference; a diagnostic.
+struct Census {
+  unsigned long long solves, ref_sides, rel_sides;
 };
 
 template <class T> inline T mx(T a, T b) { return a > b ? a : b; }
@@ -145,20 +155,28 @@ template <class T> Q<T> hll_x(const Q<T>& L, const Q<T>& R, T g, T bn, T fbn, T 
   f[5] = fbn; f[8] = fpsi; return f;
 }
 // glm_physics.jl:255-263
-template <class T> void hlld_star(T d, T u, T v, T w, T by, T bz, T S, T bn, T SM, T& ov, T& ow, T& oby, T& obz) {
+template <class T> void hlld_star(T d, T u, T v, T w, T by, T bz, T S, T bn, T SM, T dtol_rel, T& ov, T& ow, T& oby,
+                                  T& obz, Census* cen) {
   T denK = d * (S - u) * (S - SM) - bn * bn;
-  // The reference's degeneracy test is |denK| < 1e-12; it is widened here to |denK| <
-  // max(1e-12, 1e-5 bn^2), the FP32 rounding level of denK (a difference of two terms of
-  // size bn^2), as the device solver does: below it the single-star states are ~1/denK and the
-  // fan flux hinges on a 1-ulp cancellation.
-  if (std::fabs(denK) < mx(T(1e-12), T(1e-5) * bn * bn)) { ov = v; ow = w; oby = by; obz = bz; return; }
+  // The reference's degeneracy test is |denK| < 1e-12 (dtol_rel = 0). With dtol_rel = 1e-5 it
+  // is widened to |denK| < max(1e-12, 1e-5 bn^2), the FP32 rounding level of denK (a difference
+  // of two terms of size bn^2), as the device solver's relative mode does: below it the
+  // single-star states are ~1/denK and the fan flux hinges on a 1-ulp cancellation.
+  if (cen) {
+    const T a = std::fabs(denK);
+    cen->ref_sides += a < T(1e-12);
+    cen->rel_sides += a >= T(1e-12) && a < T(1e-5) * bn * bn;
+  }
+  if (std::fabs(denK) < mx(T(1e-12), dtol_rel * bn * bn)) { ov = v; ow = w; oby = by; obz = bz; return; }
   T fac = bn * (SM - u) / denK;
   ov = v - by * fac; ow = w - bz * fac;
   oby = by * (d * (S - u) * (S - u) - bn * bn) / denK;
   obz = bz * (d * (S - u) * (S - u) - bn * bn) / denK;
 }
 // glm_physics.jl:264-307
-template <class T> Q<T> hlld_x(const Q<T>& L, const Q<T>& R, T g, T bn, T fbn, T fpsi) {
+template <class T> Q<T> hlld_x(const Q<T>& L, const Q<T>& R, T g, T bn, T fbn, T fpsi, T dtol_rel,
+                               Census* cen = nullptr) {
+  if (cen) cen->solves += 1;
   T dL = L[0], uL = L[1], vL = L[2], wL = L[3], pL = L[4], byL = L[6], bzL = L[7];
   T dR = R[0], uR = R[1], vR = R[2], wR = R[3], pR = R[4], byR = R[6], bzR = R[7];
   T b2L = bn * bn + byL * byL + bzL * bzL, b2R = bn * bn + byR * byR + bzR * bzR;
@@ -178,8 +196,8 @@ template <class T> Q<T> hlld_x(const Q<T>& L, const Q<T>& R, T g, T bn, T fbn, T
   T sqdLs = std::sqrt(dLs), sqdRs = std::sqrt(dRs);
   T SLs = SM - std::fabs(bn) / sqdLs, SRs = SM + std::fabs(bn) / sqdRs;
   T vyLs, vzLs, byLs, bzLs, vyRs, vzRs, byRs, bzRs;
-  hlld_star(dL, uL, vL, wL, byL, bzL, SL, bn, SM, vyLs, vzLs, byLs, bzLs);
-  hlld_star(dR, uR, vR, wR, byR, bzR, SR, bn, SM, vyRs, vzRs, byRs, bzRs);
+  hlld_star(dL, uL, vL, wL, byL, bzL, SL, bn, SM, dtol_rel, vyLs, vzLs, byLs, bzLs, cen);
+  hlld_star(dR, uR, vR, wR, byR, bzR, SR, bn, SM, dtol_rel, vyRs, vzRs, byRs, bzRs, cen);
   T vdotbL = uL * bn + vL * byL + wL * bzL, vdotbLs = SM * bn + vyLs * byLs + vzLs * bzLs;
   T ELs = ((SL - uL) * EL - ptL * uL + pts * SM + bn * (vdotbL - vdotbLs)) / (SL - SM);
   T vdotbR = uR * bn + vR * byR + wR * bzR, vdotbRs = SM * bn + vyRs * byRs + vzRs * bzRs;
@@ -203,7 +221,7 @@ template <class T> Q<T> hlld_x(const Q<T>& L, const Q<T>& R, T g, T bn, T fbn, T
   f[5] = fbn; f[8] = fpsi; return f;
 }
 // glm_physics.jl:317-329
-template <class T> Q<T> riemann(const Q<T>& Lq, const Q<T>& Rq, int d, T ch, const Phys<T>& P) {
+template <class T> Q<T> riemann(const Q<T>& Lq, const Q<T>& Rq, int d, T ch, const Phys<T>& P, Census* cen = nullptr) {
   Q<T> L = rot_to(Lq, d), R = rot_to(Rq, d);
   L[0] = mx(L[0], P.smallr); L[4] = mx(L[4], P.pfl);
   R[0] = mx(R[0], P.smallr); R[4] = mx(R[4], P.pfl);
@@ -215,11 +233,11 @@ template <class T> Q<T> riemann(const Q<T>& Lq, const Q<T>& Rq, int d, T ch, con
   Q<T> f;
   if (P.rsol == RS_LLF) f = llf_x(L, R, P.gamma, ch, fbn, fpsi);
   else if (P.rsol == RS_HLL) f = hll_x(L, R, P.gamma, bns, fbn, fpsi);
-  else f = uself ? llf_x(L, R, P.gamma, ch, fbn, fpsi) : hlld_x(L, R, P.gamma, bns, fbn, fpsi);
+  else f = uself ? llf_x(L, R, P.gamma, ch, fbn, fpsi) : hlld_x(L, R, P.gamma, bns, fbn, fpsi, P.dtol_rel, cen);
   return rot_flux_from(f, d);
 }
 // glm_physics.jl:336-348
-template <class T> Q<T> riemann_ct(const Q<T>& Lq, const Q<T>& Rq, int d, const Phys<T>& P) {
+template <class T> Q<T> riemann_ct(const Q<T>& Lq, const Q<T>& Rq, int d, const Phys<T>& P, Census* cen = nullptr) {
   Q<T> L0 = rot_to(Lq, d), R0 = rot_to(Rq, d);
   Q<T> L = L0, R = R0;
   L[0] = mx(L0[0], P.smallr); L[4] = mx(L0[4], P.pfl); L[8] = T(0);
@@ -229,11 +247,12 @@ template <class T> Q<T> riemann_ct(const Q<T>& Lq, const Q<T>& Rq, int d, const 
   Q<T> f;
   if (P.rsol == RS_LLF) f = llf_x(L, R, P.gamma, z, z, z);
   else if (P.rsol == RS_HLL) f = hll_x(L, R, P.gamma, bns, z, z);
-  else f = uself ? llf_x(L, R, P.gamma, z, z, z) : hlld_x(L, R, P.gamma, bns, z, z);
+  else f = uself ? llf_x(L, R, P.gamma, z, z, z) : hlld_x(L, R, P.gamma, bns, z, z, P.dtol_rel, cen);
   return rot_flux_from(f, d);
 }
 
-struct Grid { int nx, ny, nz, bc[3]; };
+// zlo/zhi: the planes a Godunov step updates (zhi <= zlo: all of them)
+struct Grid { int nx, ny, nz, bc[3]; int zlo = 0, zhi = 0; };
 
 // boundary.jl:161-175 (0-based)
 inline void bcidx(int i, int n, int code, int& ii, int& flip) {
@@ -384,12 +403,19 @@ enum { W_MFX = 0, W_MFY, W_MFZ, W_FXBY, W_FXBZ, W_FYBX, W_FYBZ, W_FZBX, W_FZBY, 
 //   CT: faces (3nc, lower-face normal B) and work (W_N*nc) non-NULL.
 template <class T>
 void godunov(const Grid& g, const T* U, T* Un, T dtdx, T ch, T decay, const Phys<T>& P, T* resid,
-             const T* faces, T* work, const Drag<T>& drag, const Rad<T>& rad = Rad<T>{nullptr, 0}) {
+             const T* faces, T* work, const Drag<T>& drag, const Rad<T>& rad = Rad<T>{nullptr, 0},
+             Census* census = nullptr) {
   const long nc = (long)g.nx * g.ny * g.nz;
   const bool CT = faces != nullptr;
-#pragma omp parallel for schedule(dynamic, 64)
-  for (long c = 0; c < nc; ++c) {
+  unsigned long long n_solves = 0, n_ref = 0, n_rel = 0;
+  const long nxy = (long)g.nx * g.ny;
+  const long c0 = g.zhi > g.zlo ? (long)g.zlo * nxy : 0, c1 = g.zhi > g.zlo ? (long)g.zhi * nxy : nc;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : n_solves, n_ref, n_rel)
+  for (long c = c0; c < c1; ++c) {
     int i = (int)(c % g.nx), j = (int)((c / g.nx) % g.ny), k = (int)(c / ((long)g.nx * g.ny));
+    // census of this cell's three lower faces (each face of the grid counted once)
+    Census loc{0, 0, 0};
+    Census* cen = census ? &loc : nullptr;
     const bool fo = rad.corr != nullptr && (rad.flags & RAD_FIRST_ORDER) != 0;
     Edges<T> ec = mh_edges(g, U, nc, i, j, k, dtdx, P, fo);
     Q<T> Fl[3], Fh[3];
@@ -413,9 +439,9 @@ void godunov(const Grid& g, const T* U, T* Un, T dtdx, T ch, T decay, const Phys
         T bl = faces[d * nc + c];
         T bh = faces[d * nc + per(g, i + off[d][0], j + off[d][1], k + off[d][2])];
         Ll[5 + d] = bl; Rl[5 + d] = bl; Lh[5 + d] = bh; Rh[5 + d] = bh;
-        Fl[d] = riemann_ct(Ll, Rl, d, P); Fh[d] = riemann_ct(Lh, Rh, d, P);
+        Fl[d] = riemann_ct(Ll, Rl, d, P, cen); Fh[d] = riemann_ct(Lh, Rh, d, P);
       } else {
-        Fl[d] = riemann(Ll, Rl, d, ch, P); Fh[d] = riemann(Lh, Rh, d, ch, P);
+        Fl[d] = riemann(Ll, Rl, d, ch, P, cen); Fh[d] = riemann(Lh, Rh, d, ch, P);
       }
     }
     Q<T> U0; for (int v = 0; v < 9; ++v) U0[v] = U[v * nc + c];
@@ -476,6 +502,14 @@ void godunov(const Grid& g, const T* U, T* Un, T dtdx, T ch, T decay, const Phys
     if (bad) r[0] = -mx(std::fabs(r[0]), mx(P.smallr, P.llf_dmin));
     for (int v = 0; v < 8; ++v) Un[v * nc + c] = r[v];
     Un[8 * nc + c] = CT ? T(0) : r[8] * decay;
+    n_solves += loc.solves;
+    n_ref += loc.ref_sides;
+    n_rel += loc.rel_sides;
+  }
+  if (census) {
+    census->solves += n_solves;
+    census->ref_sides += n_ref;
+    census->rel_sides += n_rel;
   }
 }
 
@@ -628,13 +662,18 @@ struct oracle_params {
   int bc[3];
   int recon, riemann;
   double gamma, smallr, pfl, llf_dmin, llf_pmin;
+  double hlld_dtol_rel;  // 0: the reference's HLLD degeneracy test; 1e-5: the relative test
+  int zlo, zhi;          // planes a Godunov step updates (zhi <= zlo: all)
 };
 
 #define ORACLE_DEFS(T, SUF)                                                                               \
   static Phys<T> phys_##SUF(const oracle_params* p) {                                                     \
-    return Phys<T>{T(p->gamma), T(p->smallr), T(p->pfl), T(p->llf_dmin), T(p->llf_pmin), p->recon, p->riemann}; \
+    return Phys<T>{T(p->gamma), T(p->smallr), T(p->pfl), T(p->llf_dmin), T(p->llf_pmin), p->recon, p->riemann, \
+                   T(p->hlld_dtol_rel)};                                                                   \
   }                                                                                                        \
-  static Grid grid_##SUF(const oracle_params* p) { return Grid{p->nx, p->ny, p->nz, {p->bc[0], p->bc[1], p->bc[2]}}; } \
+  static Grid grid_##SUF(const oracle_params* p) {                                                      \
+    return Grid{p->nx, p->ny, p->nz, {p->bc[0], p->bc[1], p->bc[2]}, p->zlo, p->zhi};                     \
+  }                                                                                                        \
   static Drag<T> no_drag_##SUF() { return Drag<T>{false, T(0), T(0), {T(0), T(0), T(0)}}; }                 \
   static Drag<T> drag_##SUF(double q, const double* v0) {                                                  \
     Drag<T> d{true, T(0.5) * T(q), T(q), {T(0), T(0), T(0)}};                                            \
@@ -644,6 +683,13 @@ struct oracle_params {
   void oracle_step_glm_##SUF(const oracle_params* p, const T* U, T* Un, double dtdx, double ch, double decay, T* resid) { \
     godunov<T>(grid_##SUF(p), U, Un, T(dtdx), T(ch), T(decay), phys_##SUF(p), resid, nullptr, nullptr,    \
                no_drag_##SUF());                                                                  \
+  }                                                                                                        \
+  void oracle_step_glm_census_##SUF(const oracle_params* p, const T* U, T* Un, double dtdx, double ch, double decay, \
+                                    unsigned long long* out) {                                             \
+    Census cs{0, 0, 0};                                                                                    \
+    godunov<T>(grid_##SUF(p), U, Un, T(dtdx), T(ch), T(decay), phys_##SUF(p), nullptr, nullptr, nullptr,  \
+               no_drag_##SUF(), Rad<T>{nullptr, 0}, &cs);                                                  \
+    out[0] = cs.solves; out[1] = cs.ref_sides; out[2] = cs.rel_sides;                                      \
   }                                                                                                        \
   void oracle_step_glm_drag_##SUF(const oracle_params* p, const T* U, T* Un, double dtdx, double ch, double decay, \
                                   double q, const double* v0) {                                           \

@@ -25,13 +25,19 @@ RIEMANN = {"hlld": 0, "hll": 1, "llf": 2}
 BC = {"periodic": 0, "outflow": 1, "reflecting": 2}
 GLM_CR = 0.18
 N_WORK = 15
+# HLLD single-star degeneracy test |denK| < max(1e-12, dtol_rel * bn^2): 0.0 is the reference's
+# own test |denK| < 1e-12 (glm_physics.jl:257); 1e-5 is the relative test of the device
+# library's default mode.
+HLLD_DTOL_REFERENCE = 0.0
+HLLD_DTOL_RELATIVE = 1e-5
 
 
 class OracleParams(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
                 ("bc", ctypes.c_int * 3), ("recon", ctypes.c_int), ("riemann", ctypes.c_int),
                 ("gamma", ctypes.c_double), ("smallr", ctypes.c_double), ("pfl", ctypes.c_double),
-                ("llf_dmin", ctypes.c_double), ("llf_pmin", ctypes.c_double)]
+                ("llf_dmin", ctypes.c_double), ("llf_pmin", ctypes.c_double), ("hlld_dtol_rel", ctypes.c_double),
+                ("zlo", ctypes.c_int), ("zhi", ctypes.c_int)]
 
 
 def build():
@@ -50,6 +56,7 @@ def lib():
         d = ctypes.c_double
         for suf in ("f32", "f64"):
             getattr(_LIB, f"oracle_step_glm_{suf}").argtypes = [P, vp, vp, d, d, d, vp]
+            getattr(_LIB, f"oracle_step_glm_census_{suf}").argtypes = [P, vp, vp, d, d, d, vp]
             getattr(_LIB, f"oracle_step_ct_{suf}").argtypes = [P, vp, vp, vp, vp, d, vp, vp]
             getattr(_LIB, f"oracle_step_glm_drag_{suf}").argtypes = [P, vp, vp, d, d, d, d, vp]
             getattr(_LIB, f"oracle_step_ct_drag_{suf}").argtypes = [P, vp, vp, vp, vp, d, d, vp]
@@ -77,7 +84,7 @@ class OracleState:
 
     def __init__(self, dims, dx, dtype=np.float32, gamma=5 / 3, smallr=1e-6, pfl=1e-7,
                  llf_dmin=1e-4, llf_pmin=0.0, riemann="hlld", recon="plm", bcs=("periodic",) * 3,
-                 mhd_solver="glm", compensated=False):
+                 mhd_solver="glm", compensated=False, hlld_dtol_rel=HLLD_DTOL_RELATIVE):
         self.dims = tuple(int(d) for d in dims)
         self.nc = int(np.prod(self.dims))
         self.T = np.dtype(dtype).type
@@ -89,7 +96,8 @@ class OracleState:
             raise ValueError("mhd_solver='ct' requires all-periodic boundaries")
         self.p = OracleParams(self.dims[0], self.dims[1], self.dims[2], (ctypes.c_int * 3)(*[BC[b] for b in bcs]),
                               RECON[recon], RIEMANN[riemann], float(self.gamma), float(self.T(smallr)),
-                              float(self.T(pfl)), float(self.T(llf_dmin)), float(self.T(llf_pmin)))
+                              float(self.T(pfl)), float(self.T(llf_dmin)), float(self.T(llf_pmin)),
+                              float(self.T(hlld_dtol_rel)))
         self.U = np.zeros((9, self.nc), dtype=dtype)
         self.scratch = np.zeros_like(self.U)
         self.faces = np.zeros((3, self.nc), dtype=dtype) if mhd_solver == "ct" else None
@@ -115,6 +123,35 @@ class OracleState:
             self._f("step_glm")(ctypes.byref(self.p), _ptr(self.U), _ptr(self.scratch), float(dtdx),
                                 float(T(ch)), float(decay), _ptr(self.resid))
         self.U, self.scratch = self.scratch, self.U
+
+    def step_planes(self, dt, ch, zlo, zhi, glm_cr=GLM_CR):
+        """The GLM step of planes [zlo, zhi) only, written into ``scratch`` without the swap: a
+        bounded sample of a full step for timing the scheme on a large box."""
+        T = self.T
+        dtdx = T(T(dt) / self.dx)
+        decay = T(np.exp(T(-T(glm_cr) * T(ch) * T(dt) / self.dx)))
+        self.p.zlo, self.p.zhi = int(zlo), int(zhi)
+        try:
+            self._f("step_glm")(ctypes.byref(self.p), _ptr(self.U), _ptr(self.scratch), float(dtdx), float(T(ch)),
+                                float(decay), _ptr(self.resid))
+        finally:
+            self.p.zlo, self.p.zhi = 0, 0
+
+    def step_census(self, dt, ch, glm_cr=GLM_CR):
+        """One GLM step (as ``step``) that also counts, over every face once, the HLLD solves,
+        the single-star sides with |denK| < 1e-12 (the reference's degenerate branch) and those
+        with 1e-12 <= |denK| < 1e-5 bn^2 (sent to the degenerate branch only by the relative
+        test). Returns the three counts."""
+        if self.mhd_solver != "glm":
+            raise ValueError("the census step is the GLM step")
+        T = self.T
+        dtdx = T(T(dt) / self.dx)
+        decay = T(np.exp(T(-T(glm_cr) * T(ch) * T(dt) / self.dx)))
+        out = (ctypes.c_ulonglong * 3)()
+        self._f("step_glm_census")(ctypes.byref(self.p), _ptr(self.U), _ptr(self.scratch), float(dtdx),
+                                   float(T(ch)), float(decay), out)
+        self.U, self.scratch = self.scratch, self.U
+        return {"solves": int(out[0]), "ref_sides": int(out[1]), "rel_sides": int(out[2])}
 
     def step_drag_godunov(self, dt, drag_impulse, ch=None, glm_cr=GLM_CR, target_velocity=(0.0, 0.0, 0.0)):
         """Source-coupled Godunov step with linear drag (drag.jl:162-178, step_drag_godunov!;

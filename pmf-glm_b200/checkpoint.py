@@ -10,8 +10,10 @@ keeps the same content and rules in a self-describing binary container:
 
 * fields are streamed one at a time (a device array is copied to the host, written and
   released before the next), so checkpointing never holds a second full state in host memory;
-* the file is written to ``path + ".tmp"`` and renamed over ``path``, so a crash mid-write
-  leaves the previous checkpoint intact;
+* the file is written to ``path + ".tmp"``, flushed to stable storage (fsync) and renamed
+  over ``path``, so a crash or power loss mid-write leaves the previous checkpoint intact;
+* a file cut short (a copy interrupted, a full disk) is rejected with CheckpointError, not
+  half-restored;
 * restoring checks the solver (a checkpoint without an ``mhd_solver`` key is a GLM one and
   never resumes as CT, nor the other way round), the configuration fingerprint (equal, or a
   legacy subset, or only ``zend`` changed, or only explicitly allowed keys changed and accepted
@@ -54,12 +56,16 @@ def _write_block(f, obj) -> None:
     f.write(data)
 
 
-def _read_block(f):
-    raw = f.read(8)
-    if len(raw) != 8:
+def _read_exact(f, n: int) -> bytes:
+    data = f.read(n)
+    if len(data) != n:
         raise CheckpointError("truncated PMF checkpoint")
-    (n,) = struct.unpack("<Q", raw)
-    return json.loads(f.read(n).decode())
+    return data
+
+
+def _read_block(f):
+    (n,) = struct.unpack("<Q", _read_exact(f, 8))
+    return json.loads(_read_exact(f, n).decode())
 
 
 def write_pmf_checkpoint(path: str, config: dict, runtime: dict, arrays: Sequence[Tuple[str, object]]) -> int:
@@ -80,7 +86,17 @@ def write_pmf_checkpoint(path: str, config: dict, runtime: dict, arrays: Sequenc
             f.write(h.astype(dt, copy=False).tobytes())
             del h
         f.flush()
+        os.fsync(f.fileno())
     os.replace(tmp, path)
+    # the rename reaches stable storage with its directory entry (not possible everywhere)
+    try:
+        d = os.open(os.path.dirname(os.path.abspath(path)), os.O_RDONLY)
+        try:
+            os.fsync(d)
+        finally:
+            os.close(d)
+    except OSError:
+        pass
     return os.path.getsize(path)
 
 
@@ -196,7 +212,7 @@ def restore_pmf_checkpoint(path: str, expected_config: dict, arrays: Sequence[Tu
                 raise CheckpointError(f"PMF checkpoint field mismatch: stored={meta['name']} expected={expected_name}")
             dt = np.dtype(meta["dtype"])
             shape = tuple(meta["shape"])
-            data = f.read(int(np.prod(shape, dtype=np.int64)) * dt.itemsize)
+            data = _read_exact(f, int(np.prod(shape, dtype=np.int64)) * dt.itemsize)
             host = np.frombuffer(data, dtype=dt).reshape(shape)
             dshape = tuple(dest.shape)
             if shape != dshape:

@@ -51,6 +51,7 @@ int check_grid(const pmfmhd_grid* g) {
   if (!std::isfinite(g->smallr) || !std::isfinite(g->pfl) || !std::isfinite(g->llf_dmin) ||
       !std::isfinite(g->llf_pmin))
     return PMFMHD_EINVAL;
+  if (!std::isfinite(g->hlld_dtol_rel) || !(g->hlld_dtol_rel >= 0.0f)) return PMFMHD_EINVAL;
   return PMFMHD_OK;
 }
 bool all_periodic(const pmfmhd_grid* g) {
@@ -73,7 +74,9 @@ int resid_mode(float* const* r, bool* comp) {
   *comp = true;
   return PMFMHD_OK;
 }
-Phys phys_of(const pmfmhd_grid* g) { return Phys{g->gamma, g->smallr, g->pfl, g->llf_dmin, g->llf_pmin}; }
+Phys phys_of(const pmfmhd_grid* g) {
+  return Phys{g->gamma, g->smallr, g->pfl, g->llf_dmin, g->llf_pmin, g->hlld_dtol_rel};
+}
 long long ncells(const pmfmhd_grid* g) { return (long long)g->nx * g->ny * g->nz; }
 int aux_blocks(const pmfmhd_ctx* c, long long nc) {
   long long b = (nc + AUX_THREADS - 1) / AUX_THREADS;
@@ -157,9 +160,10 @@ int occupancy_of(const StepKernelInfo& k) {
   return occ;
 }
 
+// `force`: launch this instantiation (its tile height in t.ty) instead of the dispatched one.
 int launch_step(pmfmhd_ctx* c, const pmfmhd_grid* g, StepArgs& a, Tune t, bool ct, bool comp,
-                cudaStream_t s, int src = SRC_NONE) {
-  StepKernelInfo k = step_kernel_info(t.ty, g->recon, g->riemann, ct, comp, src);
+                cudaStream_t s, int src = SRC_NONE, const StepKernelInfo* force = nullptr) {
+  StepKernelInfo k = force ? *force : step_kernel_info(t.ty, g->recon, g->riemann, ct, comp, src);
   if (k.fn == nullptr) return PMFMHD_EUNSUPPORTED;
   const int occ = occupancy_of(k);
   a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
@@ -168,6 +172,7 @@ int launch_step(pmfmhd_ctx* c, const pmfmhd_grid* g, StepArgs& a, Tune t, bool c
   a.nty = (g->ny + t.ty - 1) / t.ty;
   a.P = phys_of(g);
   a.status = c->d_status;
+  a.tma_stall_polls = c->tma_stall_polls;
   a.use_tma = field_maps(c, g, a.U, t.ty, a.tmap) ? 1 : 0;
   if (a.zhi <= a.zlo) {  // the whole box unless the caller set a plane range
     a.zlo = 0;
@@ -799,6 +804,40 @@ int pmfmhd_autotune(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9]
     c->tune[TuneKey{g->nx, g->ny, g->nz, ct, comp, g->recon, g->riemann}] = best;
   }
   return result;
+}
+
+int pmfmhd_step_glm_census(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],
+                           float dt, float ch, float decay, uint64_t out[3], void* stream) {
+  if (c == nullptr || out == nullptr) return PMFMHD_EINVAL;
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!nonnull(U, 9) || !nonnull(Unew, 9)) return PMFMHD_EINVAL;
+  if (!std::isfinite(dt) || !std::isfinite(ch) || !std::isfinite(decay) || !(ch > 0.0f)) return PMFMHD_EINVAL;
+  if (g->recon != PMFMHD_RECON_PLM || g->riemann != PMFMHD_RIEMANN_HLLD) return PMFMHD_EUNSUPPORTED;
+  cudaStream_t s = as_stream(stream);
+  unsigned long long* cnt = c->d_u64 + 8;  // 64 bytes past the FP64-max cell
+  PMF_CK(cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned long long), s));
+  StepArgs a;
+  fill_glm_args(a, U, Unew, nullptr, false, dt / g->dx, ch, decay, c->d_smax);
+  a.census = cnt;
+  PMF_CK(cudaMemsetAsync(c->d_smax, 0, sizeof(unsigned int), s));
+  Tune t = tune_for(c, g, false, false);
+  t.ty = kCensusRows;
+  const StepKernelInfo k = step_census_kernel_info();
+  if ((rc = launch_step(c, g, a, t, false, false, s, SRC_NONE, &k))) return rc;
+  PMF_CK(cudaMemcpyAsync(c->h_pin, cnt, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  PMF_CK(cudaStreamSynchronize(s));
+  unsigned long long v[3];
+  std::memcpy(v, c->h_pin, sizeof(v));
+  for (int q = 0; q < 3; ++q) out[q] = (uint64_t)v[q];
+  return PMFMHD_OK;
+}
+
+int pmfmhd_set_tma_stall(pmfmhd_ctx* c, int polls) {
+  if (c == nullptr || polls < 0) return PMFMHD_EINVAL;
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->tma_stall_polls = polls;
+  return PMFMHD_OK;
 }
 
 int pmfmhd_status(pmfmhd_ctx* c, int clear, void* stream) {

@@ -22,4 +22,7 @@ constexpr int kNumTileRows = 5;
 StepKernelInfo step_kernel_info(int ty, int recon, int rsol, bool ct, bool comp, int src = 0);
 // The many-box form of the same kernel (same shared memory and block size).
 BatchKernel batch_kernel(int ty, int recon, int rsol, bool ct, bool comp);
+// The HLLD census step (8 owned rows, MC-PLM, GLM, plain update).
+StepKernelInfo step_census_kernel_info();
+constexpr int kCensusRows = 8;
 }  // namespace pmf

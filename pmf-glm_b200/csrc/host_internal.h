@@ -89,6 +89,7 @@ struct pmfmhd_ctx {
   std::map<pmf::host::MapKey, CUtensorMap> maps;  // TMA descriptors of field arrays
   unsigned int* d_status = nullptr;                // device status bits of the step kernels
   pmf::host::HostPath hp;                          // host-buffer step workspace
+  int tma_stall_polls = 0;                         // pmfmhd_set_tma_stall test hook
   std::mutex mu;
 };
 

@@ -16,10 +16,16 @@
 //   * every call shares the one array and leaves its contents behind; each call overwrites
 //     every partial it reads, so nothing needs clearing first, but calls that overlap on
 //     the GPU (two streams, two host threads) race on it and must be serialised;
-//   * the first call on a device looks up the array's device address with that device
-//     current (cudaGetSymbolAddress) and caches it; make that first call before any stream
-//     capture is active.
+//   * the first call in a CUDA context looks up the array's device address with that
+//     context current (cudaGetSymbolAddress) and caches it with the context's unique id. The
+//     array lives in the library's module, which is loaded again whenever a context is
+//     re-created (after cudaDeviceReset, or when the host application rebuilds the primary
+//     context), possibly at another address; a call that finds another context current than
+//     the cached one looks the address up again. Make the first call of each context before
+//     any stream capture is active.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cmath>
 #include <mutex>
@@ -40,8 +46,40 @@ struct FieldPtrs {
 // [kMaxPartials][8] partial sums followed by the 8 results
 static __device__ __align__(256) double g_totals_scratch[kMaxPartials * 8 + 8];
 
+// Device address of g_totals_scratch per device, valid in the context with id ctx_id.
+struct ScratchAddr {
+  unsigned long long ctx_id;
+  double* ptr;
+};
 std::mutex g_mu;
-double* g_scratch_addr[kMaxDevices] = {nullptr};
+ScratchAddr g_scratch_addr[kMaxDevices] = {};
+
+// Unique id of the calling thread's current context (cuCtxGetId: unique for the life of the
+// process, so a re-created context never repeats an old id), or 0 if there is no current
+// context or the driver entry points are unavailable. Reached through the runtime's driver
+// entry points (no link to libcuda).
+unsigned long long current_context_id() {
+  static PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
+  static PFN_cuCtxGetId_v12000 get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(p);
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(p);
+  });
+  if (get_current == nullptr || get_id == nullptr) return 0;
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return 0;
+  unsigned long long id = 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 __global__ void __launch_bounds__(kBlock) totals_block_kernel(const FieldPtrs U, int nc, double* part) {
   __shared__ double red[8][kBlock / 32];
@@ -99,12 +137,17 @@ extern "C" int pmfmhd_conserved_totals_noalloc(const pmfmhd_grid* g, const float
   double* scratch;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    if (g_scratch_addr[dev] == nullptr) {
+    ScratchAddr& slot = g_scratch_addr[dev];
+    const unsigned long long id = current_context_id();
+    if (slot.ptr == nullptr || id == 0 || id != slot.ctx_id) {
+      // set-up in this context: look the array's address up with the device current (this
+      // also creates the primary context if none is current yet), then record whose it is
       void* p = nullptr;
       if (cudaGetSymbolAddress(&p, g_totals_scratch) != cudaSuccess || p == nullptr) return PMFMHD_ECUDA;
-      g_scratch_addr[dev] = static_cast<double*>(p);
+      slot.ptr = static_cast<double*>(p);
+      slot.ctx_id = current_context_id();  // 0 if unknown: the next call looks it up again
     }
-    scratch = g_scratch_addr[dev];
+    scratch = slot.ptr;
   }
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   FieldPtrs u;

@@ -13,7 +13,9 @@
 namespace pmf {
 
 enum { RECON_PLM = 0, RECON_PPM = 1, RECON_PLM_MINMOD = 2 };
-enum { RS_HLLD = 0, RS_HLL = 1, RS_LLF = 2 };
+// RS_HLLD_CENSUS: HLLD that also counts its single-star degeneracy cases (HlldCensus); only the
+// census step instantiates it.
+enum { RS_HLLD = 0, RS_HLL = 1, RS_LLF = 2, RS_HLLD_CENSUS = 3 };
 enum { BC_PERIODIC = 0, BC_OUTFLOW = 1, BC_REFLECT = 2 };
 
 struct F9 {
@@ -24,6 +26,16 @@ struct F9 {
 
 struct Phys {
   float gamma, smallr, pfl, llf_dmin, llf_pmin;
+  // HLLD single-star degeneracy test |denK| < max(1e-12, dtol_rel * bn^2); 0 is the reference's
+  // absolute test |denK| < 1e-12 (glm_physics.jl:257)
+  float dtol_rel;
+};
+
+// Per-thread counts of the HLLD degeneracy census (RS_HLLD_CENSUS): solves, single-star sides
+// with |denK| < 1e-12 (the reference's degenerate branch) and sides with 1e-12 <= |denK| <
+// 1e-5 bn^2 (sent to the degenerate branch by the relative test only).
+struct HlldCensus {
+  unsigned solves, ref_sides, rel_sides;
 };
 
 __device__ __forceinline__ F9 add9(const F9& a, const F9& b) {
@@ -152,12 +164,14 @@ template <> struct Offsets<RECON_PPM> {
   __device__ __forceinline__ float l(int i) const { return dL[i]; }
 };
 
-// Offsets times k (k = 0: the piecewise-constant states of a first-order fallback).
-template <int RECON> __device__ __forceinline__ void scale_offsets(Offsets<RECON>& o, float k) {
+// Offsets kept or replaced by exact zeros (keep = false: the piecewise-constant states of a
+// first-order fallback). A select, not a product: an Inf or NaN offset of a bad state still
+// gives a zero offset, as the reference's assignment of zeros does (integrator_cube.jl:168-171).
+template <int RECON> __device__ __forceinline__ void keep_offsets(Offsets<RECON>& o, bool keep) {
 #pragma unroll
   for (int i = 0; i < 9; ++i) {
-    o.dR[i] *= k;
-    if constexpr (RECON == RECON_PPM) o.dL[i] *= k;
+    o.dR[i] = keep ? o.dR[i] : 0.0f;
+    if constexpr (RECON == RECON_PPM) o.dL[i] = keep ? o.dL[i] : 0.0f;
   }
 }
 
@@ -276,7 +290,8 @@ __device__ __forceinline__ F9 hll_x(const F9& L, const F9& R, float g, float bn,
 // solver are the same algebra on the two states, so they run as packed pairs (lane x = L,
 // lane y = R); the scalar parts are the wave speeds, the contact speed and the doubly-starred
 // state, which mix both sides.
-__device__ __forceinline__ F9 hlld_x(const F9& L, const F9& R, float g, float bn, float fbn, float fpsi) {
+__device__ __forceinline__ F9 hlld_x(const F9& L, const F9& R, float g, float bn, float fbn, float fpsi,
+                                     float dtol_rel, HlldCensus* cen = nullptr) {
   const float2 d = p2(L[0], R[0]), u = p2(L[1], R[1]), v = p2(L[2], R[2]), w = p2(L[3], R[3]);
   const float2 p = p2(L[4], R[4]), by = p2(L[6], R[6]), bz = p2(L[7], R[7]);
   const float2 half = pb(0.5f);
@@ -316,13 +331,19 @@ __device__ __forceinline__ F9 hlld_x(const F9& L, const F9& R, float g, float bn
   const float2 iK = p2(1.0f / denK.x, 1.0f / denK.y);
   const float2 fac = mul2(mul2(pb(bn), sub2(pb(SM), u)), iK);
   const float2 rK = mul2(nK, iK);
-  // Degenerate star state (the fast and Alfven speeds coincide): the reference tests
-  // |denK| < 1e-12, which is below the FP32 rounding of denK = d(S-u)(S-SM) - bn^2 (a
-  // difference of two terms of size bn^2); a 1-ulp residue then makes the single-star states
-  // ~1/denK and the fan flux depends on a cancellation (S*_L - S_L) * U*_L. Faces with |denK|
-  // within 1e-5 bn^2 of zero take the degenerate branch, as the oracle does.
-  const float dtol = fmaxf(1e-12f, 1e-5f * bn2);
+  // Degenerate star state (the fast and Alfven speeds coincide). The reference tests
+  // |denK| < 1e-12 (dtol_rel = 0), which is below the FP32 rounding of denK = d(S-u)(S-SM) - bn^2
+  // (a difference of two terms of size bn^2): a 1-ulp residue then makes the single-star states
+  // ~1/denK and the fan flux depends on a cancellation (S*_L - S_L) * U*_L. The relative mode
+  // (dtol_rel = 1e-5) sends faces with |denK| within 1e-5 bn^2 of zero to the degenerate branch.
+  const float dtol = fmaxf(1e-12f, dtol_rel * bn2);
   const bool degL = fabsf(denK.x) < dtol, degR = fabsf(denK.y) < dtol;
+  if (cen != nullptr) {
+    const float t5 = 1e-5f * bn2, aL = fabsf(denK.x), aR = fabsf(denK.y);
+    cen->solves += 1;
+    cen->ref_sides += (aL < 1e-12f ? 1u : 0u) + (aR < 1e-12f ? 1u : 0u);
+    cen->rel_sides += (aL >= 1e-12f && aL < t5 ? 1u : 0u) + (aR >= 1e-12f && aR < t5 ? 1u : 0u);
+  }
   float2 vs = sub2(v, mul2(by, fac)), ws = sub2(w, mul2(bz, fac));
   float2 bys = mul2(by, rK), bzs = mul2(bz, rK);
   if (degL) { vs.x = v.x; ws.x = w.x; bys.x = by.x; bzs.x = bz.x; }
@@ -370,7 +391,8 @@ __device__ __forceinline__ F9 hlld_x(const F9& L, const F9& R, float g, float bn
 // GLM Riemann problem on a D-normal face (glm_physics.jl:317-329): floors, Dedner pair,
 // the selected solver (HLLD with the LLF fallback at low density/pressure), rotate back.
 template <int D, int RSOL>
-__device__ __forceinline__ F9 riemann_glm(const F9& Lq, const F9& Rq, float ch, const Phys& P) {
+__device__ __forceinline__ F9 riemann_glm(const F9& Lq, const F9& Rq, float ch, const Phys& P,
+                                          HlldCensus* cen = nullptr) {
   F9 L = rot_to<D>(Lq), R = rot_to<D>(Rq);
   L[0] = fmaxf(L[0], P.smallr); L[4] = fmaxf(L[4], P.pfl);
   R[0] = fmaxf(R[0], P.smallr); R[4] = fmaxf(R[4], P.pfl);
@@ -387,7 +409,7 @@ __device__ __forceinline__ F9 riemann_glm(const F9& Lq, const F9& Rq, float ch, 
     bool uself = (P.llf_dmin > 0.0f && fminf(L[0], R[0]) < P.llf_dmin) ||
                  (P.llf_pmin > 0.0f && fminf(L[4], R[4]) < P.llf_pmin);
     if (uself) f = llf_x(L, R, P.gamma, ch, fbn, fpsi);
-    else f = hlld_x(L, R, P.gamma, bns, fbn, fpsi);
+    else f = hlld_x(L, R, P.gamma, bns, fbn, fpsi, P.dtol_rel, cen);
   }
   return rot_back<D>(f);
 }
@@ -395,7 +417,7 @@ __device__ __forceinline__ F9 riemann_glm(const F9& Lq, const F9& Rq, float ch, 
 // Constrained-transport Riemann problem (glm_physics.jl:336-348): the caller has put the
 // staggered face value into both states' normal-B slot; no psi, ch = 0 in the LLF speed.
 template <int D, int RSOL>
-__device__ __forceinline__ F9 riemann_ct(const F9& Lq, const F9& Rq, const Phys& P) {
+__device__ __forceinline__ F9 riemann_ct(const F9& Lq, const F9& Rq, const Phys& P, HlldCensus* cen = nullptr) {
   F9 L = rot_to<D>(Lq), R = rot_to<D>(Rq);
   L[0] = fmaxf(L[0], P.smallr); L[4] = fmaxf(L[4], P.pfl); L[8] = 0.0f;
   R[0] = fmaxf(R[0], P.smallr); R[4] = fmaxf(R[4], P.pfl); R[5] = L[5]; R[8] = 0.0f;
@@ -409,15 +431,18 @@ __device__ __forceinline__ F9 riemann_ct(const F9& Lq, const F9& Rq, const Phys&
     bool uself = (P.llf_dmin > 0.0f && fminf(L[0], R[0]) < P.llf_dmin) ||
                  (P.llf_pmin > 0.0f && fminf(L[4], R[4]) < P.llf_pmin);
     if (uself) f = llf_x(L, R, P.gamma, 0.0f, 0.0f, 0.0f);
-    else f = hlld_x(L, R, P.gamma, bns, 0.0f, 0.0f);
+    else f = hlld_x(L, R, P.gamma, bns, 0.0f, 0.0f, P.dtol_rel, cen);
   }
   return rot_back<D>(f);
 }
 
+// `cen` is read only by the census instantiation (RS_HLLD_CENSUS); pass it for the faces to be
+// counted, nullptr otherwise.
 template <int D, int RSOL, bool CT>
-__device__ __forceinline__ F9 riemann(const F9& L, const F9& R, float ch, const Phys& P) {
-  if constexpr (CT) return riemann_ct<D, RSOL>(L, R, P);
-  else return riemann_glm<D, RSOL>(L, R, ch, P);
+__device__ __forceinline__ F9 riemann(const F9& L, const F9& R, float ch, const Phys& P, HlldCensus* cen = nullptr) {
+  if constexpr (RSOL != RS_HLLD_CENSUS) cen = nullptr;
+  if constexpr (CT) return riemann_ct<D, RSOL>(L, R, P, cen);
+  else return riemann_glm<D, RSOL>(L, R, ch, P, cen);
 }
 
 // max over axes of |v_d| + c_f(B_d) of a conserved state (timestep.jl:4-14)

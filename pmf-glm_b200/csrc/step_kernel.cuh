@@ -25,6 +25,8 @@
 #pragma once
 #include <cuda.h>  // CUtensorMap (the tiled-tensor descriptor the TMA loads read)
 
+#include <type_traits>
+
 #include "physics.cuh"
 
 namespace pmf {
@@ -63,6 +65,10 @@ struct StepArgs {
   const float* dscal;       // if non-null: device {dtdx, ch, decay} overriding the values above
   unsigned int* status;     // device status bits (1: a bounded wait for a TMA load gave up), or null
   int use_tma;              // the tensor maps below describe U (fields with nx % 4 == 0)
+  int tma_stall_polls;      // test hook, normally 0: > 0 arms each TMA plane's mbarrier without
+                            // issuing its copies and gives up after this many polls, so the
+                            // bounded-wait path runs with nothing in flight
+  unsigned long long* census;  // RS_HLLD_CENSUS: solves, reference-degenerate and relative-only sides
   CUtensorMap tmap[9];      // per field: 3-D (x, y, z) FP32 map, box (PLANE_W, TY+4, 1)
   DragCoef drag;            // source-coupled steps: drag coefficients (read by SRC_DRAG/SRC_RAD kernels)
   int zlo, zhi;             // single-box launches: the planes [zlo, zhi) this launch updates
@@ -108,7 +114,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 template <int TY, int RECON, int RSOL, bool CT, bool COMP, int SRC>
 __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, int z0, int z1, float* smem,
                                              float& smax, unsigned long long* tma_bar, unsigned& tma_phase,
-                                             int* tma_off) {
+                                             int* tma_off, HlldCensus& cz) {
   constexpr bool DRAG = SRC != SRC_NONE;  // the radiation-coupled step always carries drag
   constexpr bool RAD = SRC == SRC_RAD;
   static_assert(!(DRAG && COMP), "source-coupled steps use their own remainders");
@@ -173,13 +179,17 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   // A plane whose staged box lies inside the grid comes in by TMA: one loader thread issues
   // nine tiled bulk-tensor loads (no multicast) that complete on an mbarrier. Other planes
   // (periodic wrap, outflow or reflecting ghosts) come in by per-element cp.async through the
-  // staging map.
+  // staging map. After a bounded TMA wait has given up (*tma_off set), a late copy may still
+  // land in `stage`, so the staging buffer is never touched again in this launch: every later
+  // plane is converted straight from global memory.
   const bool tma_cols = a.use_tma && (__cvta_generic_to_shared(stage) & 127) == 0 && x0 - PLANE_X0 >= 0 &&
                         x0 - PLANE_X0 + PLANE_W <= nx && y0 - 2 >= 0 && y0 + TY + 2 <= ny;
   bool pending_tma = false;  // the plane in flight came by TMA
   const unsigned bar_addr = (unsigned)__cvta_generic_to_shared(tma_bar);
   auto issue_plane = [&](int zp) {  // loaders only
-    pending_tma = tma_cols && zp >= 0 && zp < nz && *tma_off == 0;
+    pending_tma = false;
+    if (*tma_off != 0) return;  // degraded staging: convert_plane reads global memory
+    pending_tma = tma_cols && zp >= 0 && zp < nz;
     if (pending_tma) {
       if (lt == 0) {
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -187,7 +197,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
                      "r"((unsigned)(9 * S::PW * sizeof(float)))
                      : "memory");
 #pragma unroll
-        for (int f = 0; f < 9; ++f) {
+        for (int f = 0; f < 9 && a.tma_stall_polls == 0; ++f) {
           const unsigned dst = (unsigned)__cvta_generic_to_shared(stage + f * PP);
           asm volatile(
               "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
@@ -213,15 +223,17 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     cp_async_commit();
   };
   // Wait for the plane in flight (loaders only). A TMA wait is bounded: if the load never
-  // lands, the status flag is raised (the step's result is then invalid) and staging falls
-  // back to cp.async for the rest of the launch, so the kernel always finishes.
+  // lands, the status flag is raised and staging degrades to direct global loads for the rest
+  // of the launch (the plane that timed out included), so the kernel always finishes and its
+  // result is still the step's.
+  const int poll_limit = a.tma_stall_polls > 0 ? a.tma_stall_polls : (1 << 22);
   auto wait_plane = [&]() {
     if (!pending_tma) {
       cp_async_wait_all();
       return;
     }
     unsigned done = 0;
-    for (int it = 0; it < (1 << 22) && !done; ++it) {
+    for (int it = 0; it < poll_limit && !done; ++it) {
       asm volatile(
           "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
           : "=r"(done)
@@ -235,9 +247,12 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     tma_phase ^= 1u;
   };
   // Raw conserved -> primitive (reflecting walls flip the normal components first); loaders.
-  auto convert_plane = [&](int zp, float* dst) {
+  // The source is the staging buffer, or global memory once staging has degraded (one
+  // uniform branch per plane; each source has its own loop).
+  auto convert_from = [&](auto direct_tag, int zp, float* dst) {
+    constexpr bool DIRECT = decltype(direct_tag)::value;
     float fz;
-    bc_index(zp, nz, a.bc[2], &fz);
+    const int kz = bc_index(zp, nz, a.bc[2], &fz);
 #pragma unroll
     for (int k = 0; k < S::KL; ++k) {
       const int e = lt + k * S::NL;
@@ -245,8 +260,14 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
         const int fl = sidx[(2 * k + 1) * S::NL + lt];
         const float fx = (fl & 1) ? -1.0f : 1.0f, fy = (fl & 2) ? -1.0f : 1.0f;
         F9 u;
+        if constexpr (DIRECT) {
+          const int gi = kz * nxy + sidx[(2 * k) * S::NL + lt];
 #pragma unroll
-        for (int f = 0; f < 9; ++f) u[f] = stage[f * PP + e];
+          for (int f = 0; f < 9; ++f) u[f] = __ldg(a.U[f] + gi);
+        } else {
+#pragma unroll
+          for (int f = 0; f < 9; ++f) u[f] = stage[f * PP + e];
+        }
         u[1] *= fx; u[5] *= fx;
         u[2] *= fy; u[6] *= fy;
         u[3] *= fz; u[7] *= fz;
@@ -255,6 +276,10 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
         for (int f = 0; f < 9; ++f) dst[f * PP + e] = q[f];
       }
     }
+  };
+  auto convert_plane = [&](int zp, float* dst) {
+    if (*tma_off != 0) convert_from(std::true_type{}, zp, dst);
+    else convert_from(std::false_type{}, zp, dst);
   };
   // barrier among the loader warps only (named barrier 1)
   auto loader_sync = [&]() { asm volatile("bar.sync 1, %0;\n" ::"r"(S::NL) : "memory"); };
@@ -433,12 +458,12 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     oy = recon<RECON>(ld9(p0, r0 - 1, c0), m0, ld9(p0, r0 + 1, c0));
     oz = recon<RECON>(ld9(pm, r0, c0), m0, ld9(pp, r0, c0));
     if constexpr (RAD) {
-      // piecewise-constant states: offsets scaled by 0 (m0 + (+-0) == m0, so every face state
-      // and Hancock flux difference is that of zero offsets), without a branch
-      const float keep = (a.rad_flags & RAD_FIRST_ORDER) ? 0.0f : 1.0f;
-      scale_offsets(ox, keep);
-      scale_offsets(oy, keep);
-      scale_offsets(oz, keep);
+      // piecewise-constant states: every offset replaced by zero (m0 + 0 == m0, so every face
+      // state and Hancock flux difference is that of zero offsets), without a branch
+      const bool keep = (a.rad_flags & RAD_FIRST_ORDER) == 0;
+      keep_offsets(ox, keep);
+      keep_offsets(oy, keep);
+      keep_offsets(oz, keep);
     }
     {
       const F9 u0 = prim2cons(m0, g);
@@ -508,7 +533,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       if constexpr (CT) {
         L[7] = bnz; R[7] = bnz;
       }
-      const F9 Fz = riemann<2, RSOL, CT>(L, R, ch, P);
+      const F9 Fz = riemann<2, RSOL, CT>(L, R, ch, P, (own && mid) ? &cz : nullptr);
       if constexpr (CT) {
         if (own && mid) {
           a.work[2][cell_p] = Fz[0];
@@ -553,7 +578,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
         if constexpr (CT) {
           L[5] = bnx; R[5] = bnx;
         }
-        Fx = riemann<0, RSOL, CT>(L, R, ch, P);
+        Fx = riemann<0, RSOL, CT>(L, R, ch, P, own ? &cz : nullptr);
         if (halo_warp) {
 #pragma unroll
           for (int i = 0; i < 9; ++i) fxright[hrow * 9 + i] = Fx[i];
@@ -578,7 +603,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       if constexpr (CT) {
         L[6] = bny; R[6] = bny;
       }
-      const F9 Fy = riemann<1, RSOL, CT>(L, R, ch, P);
+      const F9 Fy = riemann<1, RSOL, CT>(L, R, ch, P, own ? &cz : nullptr);
 #pragma unroll
       for (int i = 0; i < 9; ++i) fybuf[((w - 1) * 9 + i) * 32 + lane] = Fy[i];
       if constexpr (CT) {
@@ -591,6 +616,35 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     }
   }
   cp_async_wait_all();
+}
+
+// After the last plane: if a bounded TMA wait gave up in this launch, give the copies of that
+// plane one more bounded wait before the CTA exits (its shared memory may not be released with
+// a bulk copy still writing into it). Every thread of the CTA calls it; thread 0, a loader,
+// tracks the barrier phase.
+__device__ __forceinline__ void drain_tma(unsigned long long* bar, unsigned tma_phase, const int* off, int polls) {
+  __syncthreads();
+  if (threadIdx.x != 0 || *off == 0) return;
+  const unsigned addr = (unsigned)__cvta_generic_to_shared(bar);
+  unsigned done = 0;
+  for (int it = 0; it < polls && !done; ++it) {
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(tma_phase ^ 1u)
+        : "memory");
+  }
+}
+
+// Census counts of the CTA summed into census[0..2] (every thread calls it).
+__device__ __forceinline__ void flush_census(const HlldCensus& cz, unsigned long long* census) {
+  unsigned long long v[3] = {cz.solves, cz.ref_sides, cz.rel_sides};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    if ((threadIdx.x & 31) == 0 && v[q] != 0) atomicAdd(census + q, v[q]);
+  }
 }
 
 // The staging mbarrier (one arrival per TMA plane, the loads' bytes as its transaction).
@@ -640,15 +694,18 @@ __global__ void __launch_bounds__(step_threads<TY>(), step_min_blocks<TY>()) mhd
   const int nzr = a.zhi - a.zlo;  // planes of this launch
   cta_range((long long)a.ntx * a.nty * nzr, &q, &qe);
   float smax = 0.0f;
+  HlldCensus cz{0u, 0u, 0u};
   while (q < qe) {
     const int col = (int)(q / nzr);
     const int zr = (int)(q - (long long)col * nzr);
     const int z0 = a.zlo + zr;
     const int z1 = a.zlo + (int)min((long long)nzr, zr + (qe - q));
     march_column<TY, RECON, RSOL, CT, COMP, SRC>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar,
-                                                  tma_phase, &tma_off);
+                                                  tma_phase, &tma_off, cz);
     q += z1 - z0;
   }
+  drain_tma(&tma_bar, tma_phase, &tma_off, a.tma_stall_polls > 0 ? a.tma_stall_polls : (1 << 22));
+  if constexpr (RSOL == RS_HLLD_CENSUS) flush_census(cz, a.census);
   if (!CT && a.smax_bits != nullptr) flush_smax<step_threads<TY>()>(smax, a.smax_bits);
 }
 
@@ -677,6 +734,7 @@ __global__ void __launch_bounds__(step_threads<TY>(), step_min_blocks<TY>()) mhd
     else hi = mid - 1;
   }
   float smax = 0.0f;
+  HlldCensus cz{0u, 0u, 0u};  // unused: the batched form has no census
   while (q < qe) {
     while (b + 1 < nbox && boxes[b + 1].q0 <= q) {
       if (!CT && boxes[b].a.smax_bits != nullptr) flush_smax<step_threads<TY>()>(smax, boxes[b].a.smax_bits);
@@ -689,9 +747,10 @@ __global__ void __launch_bounds__(step_threads<TY>(), step_min_blocks<TY>()) mhd
     const int z0 = (int)(local - (long long)col * a.nz);
     const int z1 = (int)min((long long)a.nz, z0 + (qe - q));
     march_column<TY, RECON, RSOL, CT, COMP, SRC_NONE>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar,
-                                                   tma_phase, &tma_off);
+                                                   tma_phase, &tma_off, cz);
     q += z1 - z0;
   }
+  drain_tma(&tma_bar, tma_phase, &tma_off, 1 << 22);
   if (!CT && boxes[b].a.smax_bits != nullptr) flush_smax<step_threads<TY>()>(smax, boxes[b].a.smax_bits);
 }
 

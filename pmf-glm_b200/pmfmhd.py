@@ -23,7 +23,8 @@ import numpy as np
 import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libpmfmhd.so")
+# PMFMHD_LIB overrides the library path (the same variable the Julia shim reads)
+LIB_PATH = os.environ.get("PMFMHD_LIB", os.path.join(HERE, "libpmfmhd.so"))
 
 GLM_CR = 0.18  # driver.jl:8
 NVAR = 9
@@ -32,6 +33,11 @@ RIEMANN = {"hlld": 0, "hll": 1, "llf": 2}
 BC = {"periodic": 0, "outflow": 1, "reflecting": 2}
 CT_NSLOT = 21
 FLOAT32_EPS = float(np.finfo(np.float32).eps)
+# HLLD single-star degeneracy tolerance (pmfmhd_grid.hlld_dtol_rel): the degenerate branch is
+# taken when |denK| < max(1e-12, dtol_rel * bn^2). 0.0 is the reference's own test
+# |denK| < 1e-12 (glm_physics.jl:257); 1e-5, the default here, is the relative test.
+HLLD_DTOL_REFERENCE = 0.0
+HLLD_DTOL_RELATIVE = 1e-5
 
 
 class PMFMHDError(RuntimeError):
@@ -42,7 +48,8 @@ class Grid(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
                 ("bc", ctypes.c_int32 * 3), ("recon", ctypes.c_int32), ("riemann", ctypes.c_int32),
                 ("dx", ctypes.c_float), ("gamma", ctypes.c_float), ("smallr", ctypes.c_float),
-                ("pfl", ctypes.c_float), ("llf_dmin", ctypes.c_float), ("llf_pmin", ctypes.c_float)]
+                ("pfl", ctypes.c_float), ("llf_dmin", ctypes.c_float), ("llf_pmin", ctypes.c_float),
+                ("hlld_dtol_rel", ctypes.c_float)]
 
 
 class Box(ctypes.Structure):
@@ -122,6 +129,9 @@ SIGNATURES = {
     "pmfmhd_batch_destroy": ([_VP], ctypes.c_int),
     "pmfmhd_autotune": ([_VP, _GP, _P9, ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
     "pmfmhd_status": ([_VP, ctypes.c_int, _VP], ctypes.c_int),
+    "pmfmhd_step_glm_census": ([_VP, _GP, _P9, _P9, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                ctypes.c_uint64 * 3, _VP], ctypes.c_int),
+    "pmfmhd_set_tma_stall": ([_VP, ctypes.c_int], ctypes.c_int),
     "pmfmhd_set_tile": ([_VP, _GP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "pmfmhd_get_tile": ([_VP, _GP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                          ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
@@ -236,9 +246,13 @@ def uses_ct(s: MHDState) -> bool:
 def allocate_state(dims: Sequence[int], dx: float, gamma: float = 5 / 3, smallr: float = 1e-6, pfl: float = 1e-7,
                    llf_dmin: float = 1e-4, llf_pmin: float = 0.0, use_hlld: bool = True, riemann=None,
                    bc: str = "periodic", bcs=None, recon: str = "plm", mhd_solver: str = "glm",
-                   compensated: bool = False, device: Optional[int] = None) -> MHDState:
+                   compensated: bool = False, device: Optional[int] = None,
+                   hlld_dtol_rel: float = HLLD_DTOL_RELATIVE) -> MHDState:
     """Zero-filled FP32 state on the GPU (state.jl:123-141). ``compensated`` adds the seven
-    Kahan remainder arrays of the compensated update (momentum, E, B)."""
+    Kahan remainder arrays of the compensated update (momentum, E, B). ``hlld_dtol_rel`` is
+    the HLLD degeneracy tolerance (HLLD_DTOL_REFERENCE for the reference's own test)."""
+    if not (np.isfinite(hlld_dtol_rel) and hlld_dtol_rel >= 0):
+        raise PMFMHDError("hlld_dtol_rel must be finite and non-negative")
     if mhd_solver not in ("glm", "ct"):
         raise PMFMHDError(f"unknown mhd_solver :{mhd_solver} (have :glm, :ct)")
     bcs = tuple(bcs) if bcs is not None else (bc, bc, bc)
@@ -266,7 +280,7 @@ def allocate_state(dims: Sequence[int], dx: float, gamma: float = 5 / 3, smallr:
     s = MHDState(U, sc, dims, f32(dx), f32(gamma), f32(smallr), f32(pfl), f32(llf_dmin), f32(llf_pmin), rsym, recon,
                  bcs, device, ct, resid)
     s.grid = Grid(dims[0], dims[1], dims[2], (ctypes.c_int32 * 3)(*[BC[b] for b in bcs]), RECON[recon],
-                  RIEMANN[rsym], s.dx, s.gamma, s.smallr, s.pfl, s.llf_dmin, s.llf_pmin)
+                  RIEMANN[rsym], s.dx, s.gamma, s.smallr, s.pfl, s.llf_dmin, s.llf_pmin, f32(hlld_dtol_rel))
     return s
 
 
@@ -629,6 +643,27 @@ def get_tile(s: MHDState):
                                  1 if s.resid is not None else 0, ctypes.byref(rows), ctypes.byref(planes)),
            "get_tile")
     return rows.value, planes.value
+
+
+def step_census(s: MHDState, dt: float, ch: float, decay: float) -> dict:
+    """One GLM step (as step_cube; MC-PLM with HLLD, plain update) that also counts the HLLD
+    single-star degeneracy cases over every face once: solves, sides with |denK| < 1e-12 (the
+    reference's degenerate branch) and sides with 1e-12 <= |denK| < 1e-5 bn^2 (where the
+    reference and relative tolerances give different fluxes)."""
+    if uses_ct(s) or s.resid is not None:
+        raise PMFMHDError("the census step is the plain GLM step")
+    out = (ctypes.c_uint64 * 3)()
+    _check(lib().pmfmhd_step_glm_census(context(s.device), ctypes.byref(s.grid), _p9(s.U), _p9(s.scratch),
+                                        float(dt), float(ch), float(decay), out, _stream()), "step_census")
+    s.U, s.scratch = s.scratch, s.U
+    return {"solves": int(out[0]), "ref_sides": int(out[1]), "rel_sides": int(out[2])}
+
+
+def set_tma_stall(device: Optional[int], polls: int) -> None:
+    """Test hook of the bounded TMA wait (pmfmhd_set_tma_stall): with polls > 0 the following
+    steps on this device's context arm each TMA plane without its copies and give up after
+    `polls` polls; 0 restores normal staging."""
+    _check(lib().pmfmhd_set_tma_stall(context(device), int(polls)), "set_tma_stall")
 
 
 def device_status(s: MHDState, clear: bool = True) -> int:

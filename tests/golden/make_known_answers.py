@@ -11,7 +11,9 @@ import os
 import re
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_known_answers.py <path to the pmf-glm checkout>")
+ref = sys.argv[1]
 log = open(os.path.join(ref, "docs/data/validation-cpu.log")).read()
 out = {"source": "docs/data/validation-cpu.log (test/inherited/runtests.jl)", "alfven": {}}
 for recon in ("plm", "ppm"):

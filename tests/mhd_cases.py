@@ -37,3 +37,37 @@ def alfven_L1(make_state, get_fields, totals, evolve, N, amp=0.1, p0=0.1, tfinal
     drift = {"mass": abs(t1["mass"] - t0["mass"]) / abs(t0["mass"]),
              "energy": abs(t1["energy"] - t0["energy"]) / abs(t0["energy"])}
     return L1, n, t, drift
+
+
+def near_degenerate_box(dims, delta=1e-3, eps=1e-5, seed=3, gamma=5 / 3):
+    """Uniform gas (rho 1, p 0.1) threaded by a unit field along x, so the Alfven speed (1)
+    exceeds the sound speed, with small random transverse field (rms `delta`) and velocity
+    (rms `eps`). On every x-face the fast and Alfven speeds then nearly coincide and HLLD's
+    single-star denominator denK = d(S-u)(S-SM) - bn^2 sits within ~1e-6 bn^2 of zero: the
+    faces where the reference's absolute degeneracy test and the relative one differ. Not one
+    of the reference's problems; a stress case for glm_physics.jl:255-263."""
+    nx, ny, nz = dims
+    n = nx * ny * nz
+    r = np.random.default_rng(seed)
+    rho = np.ones(n)
+    p = np.full(n, 0.1)
+    v = r.standard_normal((3, n)) * eps
+    B = np.zeros((3, n))
+    B[0] = 1.0
+    B[1] = r.standard_normal(n) * delta
+    B[2] = r.standard_normal(n) * delta
+    U = np.zeros((9, n))
+    U[0] = rho
+    U[1:4] = rho * v
+    U[4] = p / (gamma - 1) + 0.5 * rho * (v ** 2).sum(0) + 0.5 * (B ** 2).sum(0)
+    U[5:8] = B
+    return U.astype(np.float32)
+
+
+def rel_linf(cand, ref, fields=range(8)):
+    """Per-field max|cand-ref| / max|ref| (FP64 arithmetic)."""
+    out = []
+    for v in fields:
+        r = np.asarray(ref[v], dtype=np.float64)
+        out.append(float(np.abs(np.asarray(cand[v], dtype=np.float64) - r).max() / max(np.abs(r).max(), 1e-300)))
+    return out

@@ -57,8 +57,9 @@ def test_null_context_is_rejected_without_device_work():
 
 
 def test_grid_struct_layout_matches_header():
-    assert ctypes.sizeof(pmfmhd.Grid) == 4 * 14
+    assert ctypes.sizeof(pmfmhd.Grid) == 4 * 15
     assert pmfmhd.Grid.dx.offset == 32
+    assert pmfmhd.Grid.hlld_dtol_rel.offset == 56
 
 
 @pytest.mark.parametrize("kw,msg", [

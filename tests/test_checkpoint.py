@@ -86,3 +86,20 @@ def test_shape_dtype_name_and_magic_checks(tmp_path):
     with pytest.raises(CheckpointError, match="unsupported"):
         restore_pmf_checkpoint(str(tmp_path / "bad.bin"), cfg, [("a", da)])
     assert not (tmp_path / "c.bin.tmp").exists()
+
+
+def test_truncated_checkpoint_is_rejected(tmp_path):
+    """A file cut short anywhere (header, field metadata or field data) raises CheckpointError
+    rather than failing in reshape or restoring part of a state."""
+    path = str(tmp_path / "c.bin")
+    cfg = dict(N=4)
+    a = np.arange(12, dtype=np.float32).reshape(3, 4)
+    b = np.arange(5, dtype=np.float64)
+    write_pmf_checkpoint(path, cfg, {"t": 0.5}, [("a", a), ("b", b)])
+    full = open(path, "rb").read()
+    for cut in (len(full) - 1, len(full) - 5 * 8, len(full) - 45, 40):
+        bad = str(tmp_path / f"cut{cut}.bin")
+        with open(bad, "wb") as f:
+            f.write(full[:cut])
+        with pytest.raises(CheckpointError, match="truncated"):
+            restore_pmf_checkpoint(bad, cfg, [("a", np.zeros((3, 4), np.float32)), ("b", np.zeros(5, np.float64))])

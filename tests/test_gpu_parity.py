@@ -1,7 +1,11 @@
 """Parity of the CUDA library (through its C ABI) with the CPU oracle on the reference's
 own test cases. Gates follow test/test_backends.jl:65-121 (per field
 max|cand-ref| <= 2e-6 + 5e-5*max|ref|, positive density, mass drift < 3e-6) and
-test/inherited/test_ct.jl for constrained transport."""
+test/inherited/test_ct.jl for constrained transport.
+
+The scheme tests run in both HLLD degeneracy modes, each against the oracle in the same mode:
+"reference" (hlld_dtol_rel = 0, the reference's own test |denK| < 1e-12, glm_physics.jl:257)
+and "relative" (1e-5, the library's default)."""
 import numpy as np
 import pytest
 import torch
@@ -13,6 +17,9 @@ import problems
 from mhd_cases import KNOWN, alfven_L1, within_parity
 
 pytestmark = pytest.mark.gpu
+
+MODES = [pytest.param(pmfmhd.HLLD_DTOL_REFERENCE, id="reference"),
+         pytest.param(pmfmhd.HLLD_DTOL_RELATIVE, id="relative")]
 
 
 def gpu_state(U, dims, **kw):
@@ -29,14 +36,15 @@ def oracle_state(U, dims, **kw):
     return s
 
 
+@pytest.mark.parametrize("dtol", MODES)
 @pytest.mark.parametrize("recon", ["plm", "ppm", "plm_minmod"])
 @pytest.mark.parametrize("riemann", ["hlld", "hll", "llf"])
-def test_smooth_glm_matches_oracle(recon, riemann):
+def test_smooth_glm_matches_oracle(recon, riemann, dtol):
     """test_backends.jl:76-121: N=16 smooth field, 3 steps at cfl 0.08."""
     n = 16
     U = problems.smooth_fields(n)
-    cpu = oracle_state(U, (n, n, n), recon=recon, riemann=riemann)
-    dev = gpu_state(U, (n, n, n), recon=recon, riemann=riemann)
+    cpu = oracle_state(U, (n, n, n), recon=recon, riemann=riemann, hlld_dtol_rel=dtol)
+    dev = gpu_state(U, (n, n, n), recon=recon, riemann=riemann, hlld_dtol_rel=dtol)
     dt, speed = cpu.compute_dt(0.08)
     for _ in range(3):
         cpu.step(dt, ch=speed)
@@ -49,12 +57,13 @@ def test_smooth_glm_matches_oracle(recon, riemann):
     assert np.abs(host[1] - U[1]).max() > 1e-7  # the state evolved
 
 
+@pytest.mark.parametrize("dtol", MODES)
 @pytest.mark.parametrize("dims", [(37, 11, 5), (64, 8, 3), (30, 9, 17), (7, 40, 6)])
-def test_ragged_grids_match_oracle(dims):
+def test_ragged_grids_match_oracle(dims, dtol):
     """Extents that are not multiples of the CTA tile (partial tiles, short z chunks)."""
     U = problems.turb_field(dims, 1.0 / max(dims))
-    cpu = oracle_state(U, dims)
-    dev = gpu_state(U, dims)
+    cpu = oracle_state(U, dims, hlld_dtol_rel=dtol)
+    dev = gpu_state(U, dims, hlld_dtol_rel=dtol)
     dt, speed = cpu.compute_dt(0.2)
     for _ in range(4):
         cpu.step(dt, ch=speed)
@@ -62,13 +71,14 @@ def test_ragged_grids_match_oracle(dims):
     assert not within_parity(cpu.U, pmfmhd.fields_to_host(dev))
 
 
+@pytest.mark.parametrize("dtol", MODES)
 @pytest.mark.parametrize("bcs", [("outflow", "periodic", "periodic"), ("reflecting", "outflow", "reflecting"),
                                  ("periodic", "reflecting", "outflow")])
-def test_boundary_conditions_match_oracle(bcs):
+def test_boundary_conditions_match_oracle(bcs, dtol):
     dims = (40, 12, 10)
     U = problems.turb_field(dims, 1.0 / 40)
-    cpu = oracle_state(U, dims, bcs=bcs)
-    dev = gpu_state(U, dims, bcs=bcs)
+    cpu = oracle_state(U, dims, bcs=bcs, hlld_dtol_rel=dtol)
+    dev = gpu_state(U, dims, bcs=bcs, hlld_dtol_rel=dtol)
     dt, speed = cpu.compute_dt(0.2)
     for _ in range(4):
         cpu.step(dt, ch=speed)
@@ -76,11 +86,12 @@ def test_boundary_conditions_match_oracle(bcs):
     assert not within_parity(cpu.U, pmfmhd.fields_to_host(dev))
 
 
-def test_compensated_matches_oracle():
+@pytest.mark.parametrize("dtol", MODES)
+def test_compensated_matches_oracle(dtol):
     n = 24
     U = problems.smooth_fields(n)
-    cpu = oracle_state(U, (n, n, n), compensated=True)
-    dev = gpu_state(U, (n, n, n), compensated=True)
+    cpu = oracle_state(U, (n, n, n), compensated=True, hlld_dtol_rel=dtol)
+    dev = gpu_state(U, (n, n, n), compensated=True, hlld_dtol_rel=dtol)
     dt, speed = cpu.compute_dt(0.2)
     for _ in range(5):
         cpu.step(dt, ch=speed)
@@ -186,15 +197,17 @@ def test_periodic_shift_invariance():
 
 
 # ---- constrained transport -----------------------------------------------------------
+@pytest.mark.parametrize("dtol", MODES)
 @pytest.mark.parametrize("riemann", ["hlld", "hll"])
-def test_ct_matches_oracle(riemann):
+def test_ct_matches_oracle(riemann, dtol):
     """test_backends.jl:353-405: CT on the smooth field, faces from the cells."""
     n = 16
     U = problems.smooth_fields(n)
-    dev = gpu_state(U, (n, n, n), riemann=riemann, mhd_solver="ct")
+    dev = gpu_state(U, (n, n, n), riemann=riemann, mhd_solver="ct", hlld_dtol_rel=dtol)
     info = pmfmhd.ct_faces_from_cells(dev)
     assert info["max_divb_face_dx_over_brms"] < 1e-5
-    cpu = oracle_state(pmfmhd.fields_to_host(dev), (n, n, n), riemann=riemann, mhd_solver="ct")
+    cpu = oracle_state(pmfmhd.fields_to_host(dev), (n, n, n), riemann=riemann, mhd_solver="ct",
+                       hlld_dtol_rel=dtol)
     cpu.faces[:] = dev.ct.packed[: 3 * n ** 3].cpu().numpy().reshape(3, -1)
     dt, _ = cpu.compute_dt(0.08)
     for _ in range(3):
@@ -210,14 +223,15 @@ def test_ct_matches_oracle(riemann):
     assert np.all(host[8] == 0)
 
 
-def test_ct_from_potential_matches_oracle():
+@pytest.mark.parametrize("dtol", MODES)
+def test_ct_from_potential_matches_oracle(dtol):
     N = 24
     g = 5 / 3
     U = fk_port.ct_test_hydro(N, g).astype(np.float32)
     A = fk_port.ct_test_potential(N).astype(np.float32)
-    dev = gpu_state(U, (N, N, N), mhd_solver="ct", riemann="hlld")
+    dev = gpu_state(U, (N, N, N), mhd_solver="ct", riemann="hlld", hlld_dtol_rel=dtol)
     pmfmhd.ct_faces_from_potential(dev, A[0], A[1], A[2])
-    cpu = oracle_state(U, (N, N, N), mhd_solver="ct", riemann="hlld")
+    cpu = oracle_state(U, (N, N, N), mhd_solver="ct", riemann="hlld", hlld_dtol_rel=dtol)
     cpu.ct_faces_from_potential(A)
     assert not within_parity(cpu.U, pmfmhd.fields_to_host(dev))
     dt, _ = cpu.compute_dt(0.3)
@@ -245,13 +259,14 @@ def test_ct_compensated_faces_match_oracle():
     assert np.abs(rb).max() > 0
 
 
-def test_tma_staged_interior_matches_oracle_and_status_is_clear():
+@pytest.mark.parametrize("dtol", MODES)
+def test_tma_staged_interior_matches_oracle_and_status_is_clear(dtol):
     """A box large enough for TMA-staged interior tiles (x extent a multiple of 4, more than
     40 cells): the result still matches the oracle and no bounded TMA wait gave up."""
     dims = (96, 40, 24)
     U = problems.turb_field(dims, 1.0 / 96)
-    cpu = oracle_state(U, dims)
-    dev = gpu_state(U, dims)
+    cpu = oracle_state(U, dims, hlld_dtol_rel=dtol)
+    dev = gpu_state(U, dims, hlld_dtol_rel=dtol)
     pmfmhd.device_status(dev, clear=True)
     dt, speed = cpu.compute_dt(0.2)
     for _ in range(3):
@@ -265,8 +280,9 @@ def test_near_degenerate_hlld_face_stays_consistent():
     """Regression: a 96^3 piece of the 512^3 turbulent box (seed 0) around a face where the
     fast and Alfven speeds coincide to FP32 rounding. With the reference's absolute 1e-12
     degeneracy test the single-star states reach ~1e4 and the fan flux rests on a 1-ulp
-    cancellation; the device step then diverged from the FP32 oracle after 12 steps. Both now
-    take the degenerate branch within 1e-5 B_n^2 and agree."""
+    cancellation; the device step then diverged from the FP32 oracle after 12 steps. In the
+    relative mode (the default, used here) both take the degenerate branch within 1e-5 B_n^2
+    and agree."""
     import ics
     n, m, c = 512, 96, (292, 205, 2)
     U = ics.turbulent_box(n, seed=0)["U"].reshape(9, n, n, n)

@@ -35,12 +35,13 @@ def _drifting_field(dx, gamma=5 / 3, drift=(0.031, -0.017, 0.023)):
     return U.astype(np.float32)
 
 
-def _pair(mode):
+def _pair(mode, dtol=pmfmhd.HLLD_DTOL_RELATIVE):
     dx = 1.0 / max(DIMS)
     U = _drifting_field(dx)
     kw = dict(compensated=True) if mode == "compensated" else {}
     if mode == "ct":
         kw = dict(mhd_solver="ct")
+    kw["hlld_dtol_rel"] = dtol
     dev = pmfmhd.allocate_state(DIMS, dx, **kw)
     pmfmhd.set_fields(dev, U)
     if mode == "ct":
@@ -56,10 +57,13 @@ def _pair(mode):
     return dev, cpu
 
 
+@pytest.mark.parametrize("dtol", [pytest.param(pmfmhd.HLLD_DTOL_REFERENCE, id="reference"),
+                                  pytest.param(pmfmhd.HLLD_DTOL_RELATIVE, id="relative")])
 @pytest.mark.parametrize("mode", ["glm", "compensated", "ct"])
 @pytest.mark.parametrize("rows", TILE_ROWS)
-def test_tile_height_matches_oracle(rows, mode):
-    dev, cpu = _pair(mode)
+def test_tile_height_matches_oracle(rows, mode, dtol):
+    """Each height, form and HLLD degeneracy mode against the FP64 oracle in the same mode."""
+    dev, cpu = _pair(mode, dtol)
     pmfmhd.set_tile(dev, rows, 8)
     assert pmfmhd.get_tile(dev) == (rows, 8)
     dt, speed = cpu.compute_dt(0.2)

@@ -6,11 +6,15 @@ into the library instead of a context. This file is collected last on purpose: i
 a run that stops at the first failure has already run every other test.
 """
 import ctypes
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
 import torch
 
+import oracle
 import pmfmhd
 import problems
 
@@ -49,8 +53,40 @@ def test_noalloc_totals_match_the_context_entry_point_twice_in_a_row():
     assert np.array_equal(_call_noalloc(first), a1)  # same grid again: same bits
 
 
+def _oracle_totals(s, U):
+    cpu = oracle.OracleState(s.dims, s.dx)
+    cpu.U[:] = U
+    t = cpu.conserved_totals()
+    return np.array([t[k] for k in ("mass", "momx", "momy", "momz", "energy", "Bx", "By", "Bz")])
+
+
+@pytest.mark.parametrize("dims", [(40, 40, 40), (256, 256, 256)], ids=["40^3", "2^24 cells"])
+def test_noalloc_totals_match_the_oracle(dims):
+    """Directly against the oracle's FP64 totals (diagnostics.jl:44-55), up to the largest grid
+    the static scratch takes: exactly 2^24 cells, every partial-sum slot in use."""
+    rng = np.random.default_rng(5)
+    nc = int(np.prod(dims))
+    U = (rng.standard_normal((9, nc), dtype=np.float32) + np.float32(1.5))
+    s = pmfmhd.set_fields(pmfmhd.allocate_state(dims, 1.0 / dims[0]), U)
+    # FP64 sums of 2^24 values in two orders (blocks of 256 here, the oracle's OpenMP chunks)
+    # agree to ~sqrt(n) ulps; a wrong cell or block would be off by ~1e-7 of the total
+    got, want = _call_noalloc(s), _oracle_totals(s, U)
+    assert np.all(np.abs(got - want) <= 1e-10 * np.abs(want)), (got, want)
+    del s
+    torch.cuda.empty_cache()
+
+
+def test_noalloc_totals_survive_a_device_reset():
+    """The scratch address is looked up once per CUDA context: after cudaDeviceReset (a host
+    that rebuilds its context) the first call looks it up again, and the totals still match the
+    oracle. Runs in a child process without torch, so the reset ends no other allocations."""
+    r = subprocess.run([sys.executable, os.path.join(os.path.dirname(__file__), "noalloc_reset_child.py")],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
+
+
 def test_noalloc_totals_reject_grids_beyond_the_static_scratch():
-    g = pmfmhd.Grid(257, 256, 256, (ctypes.c_int32 * 3)(0, 0, 0), 0, 0, 1 / 256, 5 / 3, 1e-6, 1e-7, 1e-4, 0.0)
+    g = pmfmhd.Grid(257, 256, 256, (ctypes.c_int32 * 3)(0, 0, 0), 0, 0, 1 / 256, 5 / 3, 1e-6, 1e-7, 1e-4, 0.0, 1e-5)
     fake = pmfmhd._P9(*([0x1000] * 9))  # rejected on the host before any device access
     out = (ctypes.c_double * 8)()
     assert pmfmhd.lib().pmfmhd_conserved_totals_noalloc(ctypes.byref(g), fake, out, None) == -2
