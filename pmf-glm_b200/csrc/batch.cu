@@ -235,13 +235,32 @@ int pmfmhd_batch_create(pmfmhd_ctx* c, const pmfmhd_box* boxes, int nbox, pmfmhd
       cudaMalloc(&b->d_smax, sizeof(unsigned int) * nbox) != cudaSuccess ||
       cudaMalloc(&b->d_meta, sizeof(BoxMeta) * nbox) != cudaSuccess)
     return fail(PMFMHD_ENOMEM);
-  // groups by (solver, compensation, reconstruction, Riemann solver, tile height)
+  // Groups by (solver, compensation, reconstruction, Riemann solver). One tile height per
+  // group, the one tuned for the group's largest box: the single-box tuning of a small box
+  // favours short tiles (more CTAs for a box that cannot fill the GPU alone), but in a batch
+  // every box shares the persistent CTAs, so the taller tile's lower halo overhead wins and
+  // the step stays one launch per group.
+  std::map<std::tuple<int, int, int, int>, int> family_ty;
+  {
+    std::map<std::tuple<int, int, int, int>, long long> family_cells;
+    for (int i = 0; i < nbox; ++i) {
+      const pmfmhd_box& x = boxes[i];
+      const bool ct = x.mhd_solver == 1, comp = x.resid[0] != nullptr;
+      const auto fam = std::make_tuple((int)ct, (int)comp, x.grid.recon, x.grid.riemann);
+      const long long nc = ncells(&x.grid);
+      if (nc > family_cells[fam]) {
+        family_cells[fam] = nc;
+        family_ty[fam] = tune_for(c, &x.grid, ct, comp).ty;
+      }
+    }
+  }
   std::map<std::tuple<int, int, int, int, int>, int> gidx;
   std::vector<BoxMeta> meta(nbox);
   for (int i = 0; i < nbox; ++i) {
     const pmfmhd_box& x = boxes[i];
     const bool ct = x.mhd_solver == 1, comp = x.resid[0] != nullptr;
-    const Tune t = tune_for(c, &x.grid, ct, comp);
+    Tune t = tune_for(c, &x.grid, ct, comp);
+    t.ty = family_ty[std::make_tuple((int)ct, (int)comp, x.grid.recon, x.grid.riemann)];
     auto key = std::make_tuple((int)ct, (int)comp, x.grid.recon, x.grid.riemann, t.ty);
     if (!gidx.count(key)) {
       Group g;

@@ -390,13 +390,15 @@ __device__ __forceinline__ F9 hlld_x(const F9& L, const F9& R, float g, float bn
 
 // GLM Riemann problem on a D-normal face (glm_physics.jl:317-329): floors, Dedner pair,
 // the selected solver (HLLD with the LLF fallback at low density/pressure), rotate back.
+// ich = 1/ch, formed once per launch: the cleaned normal field every solve starts from then
+// waits on a multiply, not on a division.
 template <int D, int RSOL>
-__device__ __forceinline__ F9 riemann_glm(const F9& Lq, const F9& Rq, float ch, const Phys& P,
+__device__ __forceinline__ F9 riemann_glm(const F9& Lq, const F9& Rq, float ch, float ich, const Phys& P,
                                           HlldCensus* cen = nullptr) {
   F9 L = rot_to<D>(Lq), R = rot_to<D>(Rq);
   L[0] = fmaxf(L[0], P.smallr); L[4] = fmaxf(L[4], P.pfl);
   R[0] = fmaxf(R[0], P.smallr); R[4] = fmaxf(R[4], P.pfl);
-  float bns = 0.5f * (L[5] + R[5]) - 0.5f * (R[8] - L[8]) / ch;
+  float bns = 0.5f * (L[5] + R[5]) - 0.5f * (R[8] - L[8]) * ich;
   float psis = 0.5f * (L[8] + R[8]) - 0.5f * ch * (R[5] - L[5]);
   float fbn = psis, fpsi = ch * ch * bns;
   L[5] = bns; R[5] = bns;
@@ -439,10 +441,11 @@ __device__ __forceinline__ F9 riemann_ct(const F9& Lq, const F9& Rq, const Phys&
 // `cen` is read only by the census instantiation (RS_HLLD_CENSUS); pass it for the faces to be
 // counted, nullptr otherwise.
 template <int D, int RSOL, bool CT>
-__device__ __forceinline__ F9 riemann(const F9& L, const F9& R, float ch, const Phys& P, HlldCensus* cen = nullptr) {
+__device__ __forceinline__ F9 riemann(const F9& L, const F9& R, float ch, float ich, const Phys& P,
+                                      HlldCensus* cen = nullptr) {
   if constexpr (RSOL != RS_HLLD_CENSUS) cen = nullptr;
   if constexpr (CT) return riemann_ct<D, RSOL>(L, R, P, cen);
-  else return riemann_glm<D, RSOL>(L, R, ch, P, cen);
+  else return riemann_glm<D, RSOL>(L, R, ch, ich, P, cen);
 }
 
 // max over axes of |v_d| + c_f(B_d) of a conserved state (timestep.jl:4-14)

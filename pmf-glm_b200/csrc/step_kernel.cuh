@@ -36,7 +36,10 @@ constexpr int PLANE_W = 40; // staged plane width: x0-4 .. x0+35 (16-byte aligne
 constexpr int PLANE_X0 = 4; // column of x0 in the staged plane
 
 // Threads per CTA: TY+2 row warps and the halo warp.
-template <int TY> __host__ __device__ constexpr int step_threads() { return 32 * (TY + 3); }
+template <int TY> __host__ __device__ constexpr int step_warps() { return TY + 3; }
+template <int TY> __host__ __device__ constexpr int step_threads() { return 32 * step_warps<TY>(); }
+// The thread that issues the TMA loads and tracks the staging barrier's phase (a loader).
+template <int TY> __host__ __device__ constexpr int step_stage_lead() { return 0; }
 // CTAs per SM the step kernel is compiled for: short tiles fit two per SM (shared memory
 // under half the SM's, registers capped at 128 per thread), so one CTA's barrier waits
 // overlap the other's work.
@@ -44,11 +47,18 @@ template <int TY> __host__ __device__ constexpr int step_min_blocks() { return T
 // Registers per thread the compiler may use: each of the SM's four sub-partitions holds 16K
 // registers for the warps resident on it (ceil(warps / 4) per CTA times the CTAs per SM).
 template <int TY> __host__ __device__ constexpr int step_reg_cap() {
-  return 16384 / (32 * ((TY + 3 + 3) / 4) * step_min_blocks<TY>()) / 8 * 8;
+  return 16384 / (32 * ((step_warps<TY>() + 3) / 4) * step_min_blocks<TY>()) / 8 * 8;
 }
+
+// Two staging buffers where shared memory allows (8-10 owned rows): the next plane's load is
+// issued into the other buffer before the current one is converted, so the loaders need one
+// barrier among themselves per plane instead of two. Shorter tiles must stay under half the
+// SM's shared memory (two CTAs per SM), taller ones have no room.
+template <int TY> __host__ __device__ constexpr bool step_double_stage() { return TY >= 8 && TY <= 10; }
 
 // Number of CT workspace arrays written by the Godunov stage (reference CTState slots 4-15).
 constexpr int CT_NWORK = 12;
+
 
 struct StepArgs {
   const float* U[9];
@@ -90,6 +100,7 @@ struct StepSmem {
   static constexpr int PW = PLANE_W * PH;           // cells per staged plane
   static constexpr int PP = (PW + 31) / 32 * 32;    // field stride: 128-byte aligned for TMA
   static constexpr int STAGE = 9 * PP;              // raw conserved plane
+  static constexpr int NSTAGE = step_double_stage<TY>() ? 2 : 1;  // staging buffers
   static constexpr int PRIM = 4 * 9 * PP;           // 4-plane primitive ring
   static constexpr int YB = (TY + 1) * 9 * 32;      // y-face states / fluxes
   static constexpr int XB = TY * 9;                 // one x-face state or flux per owned row
@@ -98,7 +109,7 @@ struct StepSmem {
   static constexpr int NL = 96;                     // loader threads: warps 0, TY+1 and the halo warp
   static constexpr int KL = (PW + NL - 1) / NL;     // staged entries per loader thread
   static constexpr int SI = 2 * KL * NL;            // per loader: source (x, y) offset and flip bits
-  static constexpr int FLOATS = STAGE + PRIM + 2 * YB + 3 * XB + ZC + YL + SI;
+  static constexpr int FLOATS = NSTAGE * STAGE + PRIM + 2 * YB + 3 * XB + ZC + YL + SI;
   static constexpr size_t BYTES = sizeof(float) * FLOATS;
 };
 
@@ -121,8 +132,11 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   using S = StepSmem<TY>;
   constexpr int NT = step_threads<TY>();
   constexpr int PP = S::PP;
-  float* stage = smem;
-  float* prim = smem + S::STAGE;
+  constexpr bool DSTAGE = step_double_stage<TY>();
+  float* stage = smem;  // NSTAGE buffers of STAGE floats (each 128-byte aligned)
+  float* prim = smem + S::NSTAGE * S::STAGE;
+  // the staging buffer of plane zp (zp >= z0 - 2 >= -2)
+  auto stage_of = [&](int zp) { return DSTAGE ? stage + ((zp + 4) & 1) * S::STAGE : stage; };
   float* ybuf = prim + S::PRIM;
   float* fybuf = ybuf + S::YB;
   float* xleft = fybuf + S::YB;    // [row][9] upper x state of the left halo cell
@@ -140,6 +154,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
 
   float dtdx = a.dtdx, ch = a.ch, decay = a.decay;
   if (a.dscal != nullptr) { dtdx = a.dscal[0]; ch = a.dscal[1]; decay = a.dscal[2]; }
+  const float ich = 1.0f / ch;  // unused by CT (ch = 0)
   const Phys P = a.P;
   const float g = P.gamma;
 
@@ -154,8 +169,8 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   const bool own = row_own && x < nx && y < ny;
 
   // Staging is done by the three "loader" warps (the two y-halo rows and the halo warp),
-  // which have the least solving to do: they prefetch plane p+3 by cp.async and convert
-  // plane p+2 into the primitive ring while the owned rows solve plane p.
+  // which have the least solving to do: they prefetch plane p+3 and convert plane p+2 into
+  // the primitive ring while the owned rows solve plane p.
   const bool loader = w == 0 || w >= TY + 1;
   const int lt = w == 0 ? lane : (w == TY + 1 ? 32 + lane : 64 + lane);
   // Staging map of this column: for each staged entry e (row r, column c) a loader handles,
@@ -198,7 +213,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
                      : "memory");
 #pragma unroll
         for (int f = 0; f < 9 && a.tma_stall_polls == 0; ++f) {
-          const unsigned dst = (unsigned)__cvta_generic_to_shared(stage + f * PP);
+          const unsigned dst = (unsigned)__cvta_generic_to_shared(stage_of(zp) + f * PP);
           asm volatile(
               "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
               "[%5];\n" ::"r"(dst),
@@ -217,7 +232,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       if (e < S::PW) {
         const int gi = kz * nxy + sidx[(2 * k) * S::NL + lt];
 #pragma unroll
-        for (int f = 0; f < 9; ++f) cp_async4(stage + f * PP + e, a.U[f] + gi);
+        for (int f = 0; f < 9; ++f) cp_async4(stage_of(zp) + f * PP + e, a.U[f] + gi);
       }
     }
     cp_async_commit();
@@ -249,8 +264,10 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   // Raw conserved -> primitive (reflecting walls flip the normal components first); loaders.
   // The source is the staging buffer, or global memory once staging has degraded (one
   // uniform branch per plane; each source has its own loop).
+  const bool reflect = a.bc[0] == BC_REFLECT || a.bc[1] == BC_REFLECT || a.bc[2] == BC_REFLECT;
   auto convert_from = [&](auto direct_tag, int zp, float* dst) {
     constexpr bool DIRECT = decltype(direct_tag)::value;
+    const float* src = stage_of(zp);
     float fz;
     const int kz = bc_index(zp, nz, a.bc[2], &fz);
 #pragma unroll
@@ -266,11 +283,13 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
           for (int f = 0; f < 9; ++f) u[f] = __ldg(a.U[f] + gi);
         } else {
 #pragma unroll
-          for (int f = 0; f < 9; ++f) u[f] = stage[f * PP + e];
+          for (int f = 0; f < 9; ++f) u[f] = src[f * PP + e];
         }
-        u[1] *= fx; u[5] *= fx;
-        u[2] *= fy; u[6] *= fy;
-        u[3] *= fz; u[7] *= fz;
+        if (reflect) {  // every flip is +1 without a reflecting wall
+          u[1] *= fx; u[5] *= fx;
+          u[2] *= fy; u[6] *= fy;
+          u[3] *= fz; u[7] *= fz;
+        }
         F9 q = cons2prim(u, g, P.smallr, P.pfl);
 #pragma unroll
         for (int f = 0; f < 9; ++f) dst[f * PP + e] = q[f];
@@ -294,14 +313,24 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   // Prologue: primitives of planes z0-2, z0-1 and z0, plane z0+1 in flight.
   __syncthreads();  // the previous segment may still be reading shared memory
   if (loader) {
-    for (int zp = z0 - 2; zp <= z0; ++zp) {
-      issue_plane(zp);
-      wait_plane();
-      loader_sync();
-      convert_plane(zp, slot(zp));
-      loader_sync();
+    if constexpr (DSTAGE) {
+      issue_plane(z0 - 2);
+      for (int zp = z0 - 2; zp <= z0; ++zp) {
+        wait_plane();
+        loader_sync();
+        issue_plane(zp + 1);  // into the other buffer; zp + 1 <= z0 + 1 <= z1 + 1
+        convert_plane(zp, slot(zp));
+      }
+    } else {
+      for (int zp = z0 - 2; zp <= z0; ++zp) {
+        issue_plane(zp);
+        wait_plane();
+        loader_sync();
+        convert_plane(zp, slot(zp));
+        loader_sync();
+      }
+      if (z0 + 1 <= z1 + 1) issue_plane(z0 + 1);
     }
-    if (z0 + 1 <= z1 + 1) issue_plane(z0 + 1);
   }
 
   // Per-column carries across planes (owned rows only), in this thread's private slots of
@@ -533,7 +562,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       if constexpr (CT) {
         L[7] = bnz; R[7] = bnz;
       }
-      const F9 Fz = riemann<2, RSOL, CT>(L, R, ch, P, (own && mid) ? &cz : nullptr);
+      const F9 Fz = riemann<2, RSOL, CT>(L, R, ch, ich, P, (own && mid) ? &cz : nullptr);
       if constexpr (CT) {
         if (own && mid) {
           a.work[2][cell_p] = Fz[0];
@@ -553,9 +582,16 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     if (loader && p + 2 <= z1 + 1) {
       wait_plane();
       loader_sync();
-      convert_plane(p + 2, slot(p + 2));
-      loader_sync();
-      if (p + 3 <= z1 + 1) issue_plane(p + 3);
+      if constexpr (DSTAGE) {
+        // the other buffer was last read by convert(p+1), which every loader finished before
+        // this barrier
+        if (p + 3 <= z1 + 1) issue_plane(p + 3);
+        convert_plane(p + 2, slot(p + 2));
+      } else {
+        convert_plane(p + 2, slot(p + 2));
+        loader_sync();
+        if (p + 3 <= z1 + 1) issue_plane(p + 3);
+      }
     }
     if (!mid) continue;  // p == z0-1 or z1: only the chunk's end z-faces and update were needed
     __syncthreads();
@@ -578,7 +614,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
         if constexpr (CT) {
           L[5] = bnx; R[5] = bnx;
         }
-        Fx = riemann<0, RSOL, CT>(L, R, ch, P, own ? &cz : nullptr);
+        Fx = riemann<0, RSOL, CT>(L, R, ch, ich, P, own ? &cz : nullptr);
         if (halo_warp) {
 #pragma unroll
           for (int i = 0; i < 9; ++i) fxright[hrow * 9 + i] = Fx[i];
@@ -603,7 +639,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       if constexpr (CT) {
         L[6] = bny; R[6] = bny;
       }
-      const F9 Fy = riemann<1, RSOL, CT>(L, R, ch, P, own ? &cz : nullptr);
+      const F9 Fy = riemann<1, RSOL, CT>(L, R, ch, ich, P, own ? &cz : nullptr);
 #pragma unroll
       for (int i = 0; i < 9; ++i) fybuf[((w - 1) * 9 + i) * 32 + lane] = Fy[i];
       if constexpr (CT) {
@@ -620,11 +656,12 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
 
 // After the last plane: if a bounded TMA wait gave up in this launch, give the copies of that
 // plane one more bounded wait before the CTA exits (its shared memory may not be released with
-// a bulk copy still writing into it). Every thread of the CTA calls it; thread 0, a loader,
-// tracks the barrier phase.
-__device__ __forceinline__ void drain_tma(unsigned long long* bar, unsigned tma_phase, const int* off, int polls) {
+// a bulk copy still writing into it). Every thread of the CTA calls it; thread `lead`, a
+// loader, tracks the barrier phase.
+__device__ __forceinline__ void drain_tma(unsigned long long* bar, unsigned tma_phase, const int* off, int polls,
+                                          int lead) {
   __syncthreads();
-  if (threadIdx.x != 0 || *off == 0) return;
+  if ((int)threadIdx.x != lead || *off == 0) return;
   const unsigned addr = (unsigned)__cvta_generic_to_shared(bar);
   unsigned done = 0;
   for (int it = 0; it < polls && !done; ++it) {
@@ -704,7 +741,8 @@ __global__ void __launch_bounds__(step_threads<TY>(), step_min_blocks<TY>()) mhd
                                                   tma_phase, &tma_off, cz);
     q += z1 - z0;
   }
-  drain_tma(&tma_bar, tma_phase, &tma_off, a.tma_stall_polls > 0 ? a.tma_stall_polls : (1 << 22));
+  drain_tma(&tma_bar, tma_phase, &tma_off, a.tma_stall_polls > 0 ? a.tma_stall_polls : (1 << 22),
+            step_stage_lead<TY>());
   if constexpr (RSOL == RS_HLLD_CENSUS) flush_census(cz, a.census);
   if (!CT && a.smax_bits != nullptr) flush_smax<step_threads<TY>()>(smax, a.smax_bits);
 }
@@ -750,7 +788,7 @@ __global__ void __launch_bounds__(step_threads<TY>(), step_min_blocks<TY>()) mhd
                                                    tma_phase, &tma_off, cz);
     q += z1 - z0;
   }
-  drain_tma(&tma_bar, tma_phase, &tma_off, 1 << 22);
+  drain_tma(&tma_bar, tma_phase, &tma_off, 1 << 22, step_stage_lead<TY>());
   if (!CT && boxes[b].a.smax_bits != nullptr) flush_smax<step_threads<TY>()>(smax, boxes[b].a.smax_bits);
 }
 

@@ -22,7 +22,7 @@ struct PortArgs {
   const float* U[9];
   float* Un[9];
   int nx, ny, nz;
-  float dtdx, ch, decay;
+  float dtdx, ch, ich, decay;
   Phys P;
 };
 
@@ -67,11 +67,11 @@ __device__ __forceinline__ void axis_fluxes(const PortArgs& a, int i, int j, int
   const int di = D == 0, dj = D == 1, dk = D == 2;
   {
     const Edges em = mh_edges(a, i - di, j - dj, k - dk);
-    Fl = riemann<D, RS_HLLD, false>(face_hi<RECON_PLM>(em.mh, em.o[D]), face_lo<RECON_PLM>(ec.mh, ec.o[D]), a.ch, a.P);
+    Fl = riemann<D, RS_HLLD, false>(face_hi<RECON_PLM>(em.mh, em.o[D]), face_lo<RECON_PLM>(ec.mh, ec.o[D]), a.ch, a.ich, a.P);
   }
   {
     const Edges ep = mh_edges(a, i + di, j + dj, k + dk);
-    Fh = riemann<D, RS_HLLD, false>(face_hi<RECON_PLM>(ec.mh, ec.o[D]), face_lo<RECON_PLM>(ep.mh, ep.o[D]), a.ch, a.P);
+    Fh = riemann<D, RS_HLLD, false>(face_hi<RECON_PLM>(ec.mh, ec.o[D]), face_lo<RECON_PLM>(ep.mh, ep.o[D]), a.ch, a.ich, a.P);
   }
 }
 
@@ -117,7 +117,7 @@ extern "C" int pmfport_step_glm(const pmfmhd_grid* g, const float* const U[9], f
     a.Un[f] = Unew[f];
   }
   a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
-  a.dtdx = dt / g->dx; a.ch = ch; a.decay = decay;
+  a.dtdx = dt / g->dx; a.ch = ch; a.ich = 1.0f / ch; a.decay = decay;
   a.P = Phys{g->gamma, g->smallr, g->pfl, g->llf_dmin, g->llf_pmin, g->hlld_dtol_rel};
   const long long nc = (long long)g->nx * g->ny * g->nz;
   plain_port_kernel<<<(unsigned)((nc + 255) / 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(a);
