@@ -43,6 +43,11 @@ def parse():
                     help="time only the drag-coupled GLM step (SRC_DRAG) of the --n box")
     ap.add_argument("--compensated-only", action="store_true",
                     help="time only the compensated GLM step of the --n box (for kernel profiling)")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="time only the batched 64-box mix (--warmup graph-recording steps, then --steps steps)")
+    ap.add_argument("--rows", type=int, default=0,
+                    help="pin the step kernel's tile height (owned rows per CTA) instead of autotuning it, "
+                         "e.g. for a profiler capture whose launch order must not depend on the autotuner")
     return ap.parse_args()
 
 
@@ -117,7 +122,10 @@ def ct_only(args):
     c = pmfmhd.set_fields(pmfmhd.allocate_state((n, n, n), 1.0 / n, mhd_solver="ct"), boxc["U"])
     pmfmhd.ct_faces_from_potential(c, *boxc["A_edge"])
     dtc, _ = pmfmhd.compute_dt(c, 0.2)
-    pmfmhd.autotune(c)
+    if args.rows:
+        pmfmhd.set_tile(c, args.rows, 16)
+    else:
+        pmfmhd.autotune(c)
     for _ in range(args.warmup):
         pmfmhd.step(c, dtc, integrator="ref")
     torch.cuda.synchronize()
@@ -133,6 +141,41 @@ def ct_only(args):
     print(json.dumps({"ct_only": True, "n": n, "steps": args.steps, "ms_per_step": ms,
                       "value": n ** 3 / (ms / 1e3), "unit": UNIT, "tile": list(pmfmhd.get_tile(c)),
                       "finite": bool(np.isfinite(host).all())}))
+
+
+def batched_only(args):
+    """The batched 64-box mix alone: the boxes of `batched_mix`, tiles autotuned per (N, solver)
+    or pinned with --rows, --warmup steps (they record the graphs) then --steps timed steps; one
+    JSON line with the device time per batch step."""
+    import torch
+
+    import ics
+    import pmfmhd
+    specs = ics.batch_mix(64)
+    states = build_boxes(specs)
+    seen = set()
+    for s, sp in zip(states, specs):
+        key = (sp["n"], sp["ct"])
+        if key not in seen:
+            if args.rows:
+                pmfmhd.set_tile(s, args.rows, 16)
+            else:
+                pmfmhd.autotune(s)
+            seen.add(key)
+    b = pmfmhd.Batch(states, cfl=0.2)
+    b.step(max(2, args.warmup))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    b.step(args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    finite = all(np.isfinite(b.current_fields(i)).all() for i in range(len(states)))
+    b.close()
+    cells = sum(sp["n"] ** 3 for sp in specs)
+    print(json.dumps({"batched_only": True, "boxes": len(specs), "cells": cells, "steps": args.steps,
+                      "ms_per_step": ms, "value": cells / (ms / 1e3), "unit": UNIT, "finite": bool(finite)}))
 
 
 def workload_config(n, steps):
@@ -645,6 +688,9 @@ def main():
     if args.compensated_only:
         compensated_only(args)
         return
+    if args.batched_only:
+        batched_only(args)
+        return
     import torch
     import torch.distributed as dist
 
@@ -664,7 +710,10 @@ def main():
     s = pmfmhd.set_fields(pmfmhd.allocate_state((n, n, n), 1.0 / n, recon="plm", riemann="hlld"), U_host)
     dt, sp = pmfmhd.compute_dt(s, 0.2)
     decay = float(np.exp(np.float32(np.float32(np.float32(-0.18) * np.float32(sp)) * np.float32(dt)) / np.float32(s.dx)))
-    pmfmhd.autotune(s)
+    if args.rows:
+        pmfmhd.set_tile(s, args.rows, 16)
+    else:
+        pmfmhd.autotune(s)
 
     sampler = ClockSampler(local)
     stream = torch.cuda.current_stream()
