@@ -313,7 +313,7 @@ int pmfmhd_set_tma_stall(pmfmhd_ctx* ctx, int polls);
 int pmfmhd_status(pmfmhd_ctx* ctx, int clear, void* stream);
 
 /* Pin (or query) the tile used for this grid/solver/mode on this context: `rows` owned rows
- * per CTA (an instantiated height: 5, 8, 9, 10 or 13) and `planes` z-planes per CTA chunk. */
+ * per CTA (an instantiated height: 5, 8, 9 or 13) and `planes` z-planes per CTA chunk. */
 int pmfmhd_set_tile(pmfmhd_ctx* ctx, const pmfmhd_grid* g, int mhd_solver, int compensated, int rows, int planes);
 int pmfmhd_get_tile(pmfmhd_ctx* ctx, const pmfmhd_grid* g, int mhd_solver, int compensated, int* rows,
                     int* planes);

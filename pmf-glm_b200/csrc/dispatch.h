@@ -15,8 +15,8 @@ struct StepKernelInfo {
 };
 
 // Rows per CTA that are instantiated (tile candidates for the autotuner).
-constexpr int kTileRows[] = {5, 8, 9, 10, 13};
-constexpr int kNumTileRows = 5;
+constexpr int kTileRows[] = {5, 8, 9, 13};
+constexpr int kNumTileRows = 4;
 
 // `src`: SRC_NONE, or a source-coupled step (SRC_DRAG, SRC_RAD; `comp` must be false).
 StepKernelInfo step_kernel_info(int ty, int recon, int rsol, bool ct, bool comp, int src = 0);

@@ -50,11 +50,11 @@ template <int TY> __host__ __device__ constexpr int step_reg_cap() {
   return 16384 / (32 * ((step_warps<TY>() + 3) / 4) * step_min_blocks<TY>()) / 8 * 8;
 }
 
-// Two staging buffers where shared memory allows (8-10 owned rows): the next plane's load is
+// Two staging buffers where shared memory allows (8 and 9 owned rows): the next plane's load is
 // issued into the other buffer before the current one is converted, so the loaders need one
 // barrier among themselves per plane instead of two. Shorter tiles must stay under half the
 // SM's shared memory (two CTAs per SM), taller ones have no room.
-template <int TY> __host__ __device__ constexpr bool step_double_stage() { return TY >= 8 && TY <= 10; }
+template <int TY> __host__ __device__ constexpr bool step_double_stage() { return TY == 8 || TY == 9; }
 
 // Number of CT workspace arrays written by the Godunov stage (reference CTState slots 4-15).
 constexpr int CT_NWORK = 12;

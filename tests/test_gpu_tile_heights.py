@@ -20,7 +20,7 @@ from mhd_cases import within_parity
 
 pytestmark = pytest.mark.gpu
 
-TILE_ROWS = (5, 8, 9, 10, 13)
+TILE_ROWS = (5, 8, 9, 13)
 DIMS = (37, 29, 11)
 
 
