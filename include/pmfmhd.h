@@ -152,6 +152,7 @@ int pmfmhd_step_ct_drag(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* cons
 #define PMFMHD_RAD_CHECK_ADMISSIBILITY 8   /* write -max(|rho|, max(smallr, llf_dmin)) for rejected cells */
 #define PMFMHD_RAD_ROBUST_FALLBACK 16      /* minmod PLM with HLL on every face */
 #define PMFMHD_RAD_GLOBAL_FALLBACK 32      /* piecewise-constant states and LLF on every face, with the admissibility check */
+#define PMFMHD_RAD_MASKED_FALLBACK 64      /* per-cell mask in slot 4: masked cells piecewise constant, their faces LLF */
 /*
  * Radiation-coupled step: the drag step (target at rest, impulse drag_impulse) whose face
  * states also carry a per-cell velocity correction, with optional tracking of the density
@@ -164,12 +165,31 @@ int pmfmhd_step_ct_drag(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* cons
  * the CT cell EMF velocity), slot 4 receives the density increments, slots 5-7 and 8 are
  * the remainders of cell B (GLM) and E. For CT states (ct_packed non-null) ch and decay are
  * ignored and the faces are compensated when PMFMHD_RAD_TRACK_MAGNETIC is set. Requires
- * all-periodic boundaries. The masked per-face LLF fallback of the cube kernel
- * (`fallback=true`, integrator_cube.jl:68-83) is not provided.
+ * all-periodic boundaries.
+ * PMFMHD_RAD_MASKED_FALLBACK is the cube kernel's masked fallback (`fallback=true`, launched
+ * with CHECK == 2, integrator_cube.jl:68-83,168-171,527): slot 4 of `correction` is read as a
+ * per-cell mask; a cell whose entry is positive takes zero reconstruction offsets, a face
+ * with such a cell on either side is solved by LLF (HLLD or HLL elsewhere), and the
+ * admissibility check is on. The mask is the slot's content when the call is made: with
+ * PMFMHD_RAD_TRACK_DENSITY as well (the reference accumulates the density increments into
+ * the same slot during the launch) it is first copied into a context workspace, allocated on
+ * the first such call. PMFMHD_RAD_GLOBAL_FALLBACK takes precedence over it, as CHECK == 3
+ * does in the reference. GLM states only (the cube integrators do not run CT states):
+ * PMFMHD_EUNSUPPORTED with ct_packed.
  */
 int pmfmhd_step_radiation(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* const U[9], float* const Unew[9],
                           float* ct_packed, float* correction, float dt, float ch, float decay, float drag_impulse,
                           int flags, void* stream);
+/*
+ * Fallback mask of the masked radiation step (`_radiation_fallback_mask_k!` and
+ * `_radiation_expand_fallback_mask_k!`, radiation_coupling.jl:1536-1577): mask_out[c] = 1 if the
+ * trial density of cell c or of one of its six face neighbours (periodic) is negative, or, with
+ * mask_in non-null, if mask_in is positive there; 0 otherwise. mask_out must not overlap
+ * trial_rho or mask_in. The reference's kernels need a cubic box; any periodic box is accepted
+ * here (all-periodic boundaries required).
+ */
+int pmfmhd_radiation_fallback_mask(pmfmhd_ctx* ctx, const pmfmhd_grid* g, const float* trial_rho,
+                                   const float* mask_in, float* mask_out, void* stream);
 /*
  * In-place exact linear drag with velocity decay factor `decay` in [0, 1]
  * (`apply_linear_drag!`, drag.jl:78-117): m <- rho v0 + (m - rho v0) decay with

@@ -221,7 +221,10 @@ template <class T> Q<T> hlld_x(const Q<T>& L, const Q<T>& R, T g, T bn, T fbn, T
   f[5] = fbn; f[8] = fpsi; return f;
 }
 // glm_physics.jl:317-329
-template <class T> Q<T> riemann(const Q<T>& Lq, const Q<T>& Rq, int d, T ch, const Phys<T>& P, Census* cen = nullptr) {
+// force_llf: LLF on this face whatever P.rsol, the masked fallback of the cube kernel
+// (_cube_masked_riemann, integrator_cube.jl:68-79)
+template <class T> Q<T> riemann(const Q<T>& Lq, const Q<T>& Rq, int d, T ch, const Phys<T>& P, Census* cen = nullptr,
+                                bool force_llf = false) {
   Q<T> L = rot_to(Lq, d), R = rot_to(Rq, d);
   L[0] = mx(L[0], P.smallr); L[4] = mx(L[4], P.pfl);
   R[0] = mx(R[0], P.smallr); R[4] = mx(R[4], P.pfl);
@@ -231,13 +234,14 @@ template <class T> Q<T> riemann(const Q<T>& Lq, const Q<T>& Rq, int d, T ch, con
   L[5] = bns; R[5] = bns;
   bool uself = (P.llf_dmin > T(0) && mn(L[0], R[0]) < P.llf_dmin) || (P.llf_pmin > T(0) && mn(L[4], R[4]) < P.llf_pmin);
   Q<T> f;
-  if (P.rsol == RS_LLF) f = llf_x(L, R, P.gamma, ch, fbn, fpsi);
+  if (P.rsol == RS_LLF || force_llf) f = llf_x(L, R, P.gamma, ch, fbn, fpsi);
   else if (P.rsol == RS_HLL) f = hll_x(L, R, P.gamma, bns, fbn, fpsi);
   else f = uself ? llf_x(L, R, P.gamma, ch, fbn, fpsi) : hlld_x(L, R, P.gamma, bns, fbn, fpsi, P.dtol_rel, cen);
   return rot_flux_from(f, d);
 }
 // glm_physics.jl:336-348
-template <class T> Q<T> riemann_ct(const Q<T>& Lq, const Q<T>& Rq, int d, const Phys<T>& P, Census* cen = nullptr) {
+template <class T> Q<T> riemann_ct(const Q<T>& Lq, const Q<T>& Rq, int d, const Phys<T>& P, Census* cen = nullptr,
+                                   bool force_llf = false) {
   Q<T> L0 = rot_to(Lq, d), R0 = rot_to(Rq, d);
   Q<T> L = L0, R = R0;
   L[0] = mx(L0[0], P.smallr); L[4] = mx(L0[4], P.pfl); L[8] = T(0);
@@ -245,7 +249,7 @@ template <class T> Q<T> riemann_ct(const Q<T>& Lq, const Q<T>& Rq, int d, const 
   T bns = L[5]; T z = T(0);
   bool uself = (P.llf_dmin > z && mn(L[0], R[0]) < P.llf_dmin) || (P.llf_pmin > z && mn(L[4], R[4]) < P.llf_pmin);
   Q<T> f;
-  if (P.rsol == RS_LLF) f = llf_x(L, R, P.gamma, z, z, z);
+  if (P.rsol == RS_LLF || force_llf) f = llf_x(L, R, P.gamma, z, z, z);
   else if (P.rsol == RS_HLL) f = hll_x(L, R, P.gamma, bns, z, z);
   else f = uself ? llf_x(L, R, P.gamma, z, z, z) : hlld_x(L, R, P.gamma, bns, z, z, P.dtol_rel, cen);
   return rot_flux_from(f, d);
@@ -377,10 +381,16 @@ template <class T> Q<T> drag_correct_conserved(const Q<T>& u0, const Q<T>& trial
 // the velocity corrections added to every face state, slot 4 the accumulated density
 // increment (track_density), slots 5-7 the Kahan remainders of cell B (track_magnetic,
 // GLM only) and slot 8 that of E (track_energy).
-enum { RAD_TRACK_DENSITY = 1, RAD_TRACK_MAGNETIC = 2, RAD_TRACK_ENERGY = 4, RAD_CHECK = 8, RAD_FIRST_ORDER = 16 };
+// RAD_MASKED: the cube kernel's masked fallback (CHECK == 2, integrator_cube.jl:68-83,168-171):
+// a cell whose mask entry is positive takes zero offsets, and a face with such a cell on either
+// side takes LLF. The mask is slot 4 as it was before the step (`mask` holds that copy: the
+// density increments of the same step land in slot 4).
+enum { RAD_TRACK_DENSITY = 1, RAD_TRACK_MAGNETIC = 2, RAD_TRACK_ENERGY = 4, RAD_CHECK = 8, RAD_FIRST_ORDER = 16,
+       RAD_MASKED = 32 };
 template <class T> struct Rad {
   T* corr;   // null: no radiation coupling
   int flags;
+  const T* mask = nullptr;  // RAD_MASKED: the per-cell mask
 };
 // integrator_cube.jl:108-124
 template <class T> bool inadmissible(const Q<T>& r, const Phys<T>& P) {
@@ -417,12 +427,17 @@ void godunov(const Grid& g, const T* U, T* Un, T dtdx, T ch, T decay, const Phys
     Census loc{0, 0, 0};
     Census* cen = census ? &loc : nullptr;
     const bool fo = rad.corr != nullptr && (rad.flags & RAD_FIRST_ORDER) != 0;
-    Edges<T> ec = mh_edges(g, U, nc, i, j, k, dtdx, P, fo);
+    const bool msk = rad.corr != nullptr && (rad.flags & RAD_MASKED) != 0;
+    // masked fallback: the mask of the cell at periodic offset (di, dj, dk) from this one
+    auto masked_at = [&](int di, int dj, int dk) { return msk && rad.mask[per(g, i + di, j + dj, k + dk)] > T(0); };
+    Edges<T> ec = mh_edges(g, U, nc, i, j, k, dtdx, P, fo || masked_at(0, 0, 0));
     Q<T> Fl[3], Fh[3];
     const int off[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
     for (int d = 0; d < 3; ++d) {
-      Edges<T> em = mh_edges(g, U, nc, i - off[d][0], j - off[d][1], k - off[d][2], dtdx, P, fo);
-      Edges<T> ep = mh_edges(g, U, nc, i + off[d][0], j + off[d][1], k + off[d][2], dtdx, P, fo);
+      const bool mm = masked_at(-off[d][0], -off[d][1], -off[d][2]), m0 = masked_at(0, 0, 0);
+      const bool mp = masked_at(off[d][0], off[d][1], off[d][2]);
+      Edges<T> em = mh_edges(g, U, nc, i - off[d][0], j - off[d][1], k - off[d][2], dtdx, P, fo || mm);
+      Edges<T> ep = mh_edges(g, U, nc, i + off[d][0], j + off[d][1], k + off[d][2], dtdx, P, fo || mp);
       // face states mh + offset, drag-propagated when drag is on, plus the radiation velocity
       // correction of the owning cell (integrator_ref.jl:28-39)
       auto face = [&](const Edges<T>& e, const Q<T>& off, long cell) {
@@ -439,9 +454,9 @@ void godunov(const Grid& g, const T* U, T* Un, T dtdx, T ch, T decay, const Phys
         T bl = faces[d * nc + c];
         T bh = faces[d * nc + per(g, i + off[d][0], j + off[d][1], k + off[d][2])];
         Ll[5 + d] = bl; Rl[5 + d] = bl; Lh[5 + d] = bh; Rh[5 + d] = bh;
-        Fl[d] = riemann_ct(Ll, Rl, d, P, cen); Fh[d] = riemann_ct(Lh, Rh, d, P);
+        Fl[d] = riemann_ct(Ll, Rl, d, P, cen, mm || m0); Fh[d] = riemann_ct(Lh, Rh, d, P, nullptr, m0 || mp);
       } else {
-        Fl[d] = riemann(Ll, Rl, d, ch, P, cen); Fh[d] = riemann(Lh, Rh, d, ch, P);
+        Fl[d] = riemann(Ll, Rl, d, ch, P, cen, mm || m0); Fh[d] = riemann(Lh, Rh, d, ch, P, nullptr, m0 || mp);
       }
     }
     Q<T> U0; for (int v = 0; v < 9; ++v) U0[v] = U[v * nc + c];
@@ -704,8 +719,12 @@ struct oracle_params {
   }                                                                                                        \
   void oracle_step_glm_rad_##SUF(const oracle_params* p, const T* U, T* Un, double dtdx, double ch, double decay,  \
                                  double q, T* corr, int flags) {                                          \
-    godunov<T>(grid_##SUF(p), U, Un, T(dtdx), T(ch), T(decay), phys_##SUF(p), nullptr, nullptr, nullptr,  \
-               drag_##SUF(q, nullptr), Rad<T>{corr, flags});                                               \
+    Grid g = grid_##SUF(p);                                                                               \
+    const long nc = (long)g.nx * g.ny * g.nz;                                                             \
+    std::vector<T> mask((flags & RAD_MASKED) ? corr + 4 * nc : corr,                                       \
+                        (flags & RAD_MASKED) ? corr + 5 * nc : corr);                                      \
+    godunov<T>(g, U, Un, T(dtdx), T(ch), T(decay), phys_##SUF(p), nullptr, nullptr, nullptr,              \
+               drag_##SUF(q, nullptr), Rad<T>{corr, flags, mask.data()});                                  \
   }                                                                                                        \
   void oracle_step_ct_rad_##SUF(const oracle_params* p, const T* U, T* Un, T* faces, T* work, T* face_resid, \
                                 double dtdx, double q, T* corr, int flags) {                              \

@@ -172,23 +172,30 @@ class OracleState:
         self.U, self.scratch = self.scratch, self.U
 
     RAD_TRACK_DENSITY, RAD_TRACK_MAGNETIC, RAD_TRACK_ENERGY, RAD_CHECK, RAD_FIRST_ORDER = 1, 2, 4, 8, 16
+    RAD_MASKED = 32
 
     def step_radiation(self, dt, drag_impulse, correction, ch=0.0, decay=1.0, track_density=True,
                        track_magnetic=True, track_energy=True, check_admissibility=False, robust_fallback=False,
-                       global_fallback=False):
+                       global_fallback=False, fallback=False):
         """The radiation-coupled step kernel: step_ref_radiation! (integrator_ref.jl:238-258) and
         step_cube_radiation! (integrator_cube.jl:504-540). ``correction`` is the packed (9, nc)
         buffer of the state precision; its slot 0 is read as psi, slots 4-8 are updated.
         robust_fallback: minmod PLM with HLL; global_fallback: piecewise-constant states and LLF
         on every face, with the admissibility flag (CHECK == 3, integrator_cube.jl:168-177,
-        524-529)."""
+        524-529); fallback: the masked fallback (CHECK == 2, integrator_cube.jl:68-83,168-171):
+        slot 4 as it is before the step is a per-cell mask, masked cells take zero offsets and
+        faces touching them LLF, with the admissibility flag. The global fallback takes
+        precedence (integrator_cube.jl:527)."""
         T = self.T
         corr = correction
         assert corr.dtype == self.U.dtype and corr.shape == (9, self.nc) and corr.flags["C_CONTIGUOUS"]
+        masked = fallback and not global_fallback
+        assert not (masked and self.mhd_solver == "ct"), "the masked fallback is a cube-kernel (GLM) mode"
         flags = ((self.RAD_TRACK_DENSITY if track_density else 0) | (self.RAD_TRACK_MAGNETIC if track_magnetic else 0)
                  | (self.RAD_TRACK_ENERGY if track_energy else 0)
-                 | (self.RAD_CHECK if (check_admissibility or global_fallback) else 0)
-                 | (self.RAD_FIRST_ORDER if global_fallback else 0))
+                 | (self.RAD_CHECK if (check_admissibility or global_fallback or masked) else 0)
+                 | (self.RAD_FIRST_ORDER if global_fallback else 0)
+                 | (self.RAD_MASKED if masked else 0))
         saved = (self.p.recon, self.p.riemann)
         if robust_fallback:
             self.p.recon, self.p.riemann = RECON["plm_minmod"], RIEMANN["hll"]
@@ -307,3 +314,20 @@ class OracleState:
                                            float(self.dx))
         if self.face_resid is not None:
             self.face_resid[:] = 0
+
+
+def fallback_mask(trial_rho, dims, mask_in=None):
+    """Fallback mask of the masked radiation step, in numpy: 1 where the trial density of the
+    cell or of one of its six periodic face neighbours is negative (_radiation_fallback_mask_k!,
+    radiation_coupling.jl:1536-1552), or, with ``mask_in``, where that mask is positive there
+    as well (_radiation_expand_fallback_mask_k!, :1554-1577); 0 elsewhere. ``trial_rho`` and
+    ``mask_in`` are flat in the SoA cell order (x fastest)."""
+    nx, ny, nz = dims
+    rho = np.asarray(trial_rho).reshape(nz, ny, nx)
+    bad = rho < 0
+    if mask_in is not None:
+        bad = bad | (np.asarray(mask_in).reshape(nz, ny, nx) > 0)
+    out = bad.copy()
+    for axis in range(3):
+        out |= np.roll(bad, 1, axis=axis) | np.roll(bad, -1, axis=axis)
+    return out.astype(np.asarray(trial_rho).dtype).ravel()

@@ -230,6 +230,7 @@ struct SourceTerms {
   DragCoef drag{};
   float* corr = nullptr;
   int rad_flags = 0;
+  const float* mask = nullptr;  // masked fallback: the per-cell mask the kernel reads
 };
 
 void apply_sources(StepArgs& a, const SourceTerms* st) {
@@ -237,6 +238,7 @@ void apply_sources(StepArgs& a, const SourceTerms* st) {
   a.drag = st->drag;
   a.corr = st->corr;
   a.rad_flags = st->rad_flags;
+  a.mask = st->mask;
 }
 
 int enqueue_glm(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* const U[9], float* const Un[9], float dt,
@@ -351,6 +353,7 @@ int pmfmhd_destroy(pmfmhd_ctx* c) {
   cudaFree(c->d_status);
   cudaFreeHost(c->h_pin);
   cudaFree(c->hp.dev);
+  cudaFree(c->d_mask);
   for (auto& e : c->hp.ev) cudaEventDestroy(e);
   if (c->hp.start) cudaEventDestroy(c->hp.start);
   for (auto& st : c->hp.s)
@@ -517,10 +520,13 @@ int pmfmhd_step_radiation(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* cons
     if (U[f] == nullptr) return PMFMHD_EINVAL;
   if (!nonnull(Unew, 9)) return PMFMHD_EINVAL;
   if (flags & ~(PMFMHD_RAD_TRACK_DENSITY | PMFMHD_RAD_TRACK_MAGNETIC | PMFMHD_RAD_TRACK_ENERGY |
-                PMFMHD_RAD_CHECK_ADMISSIBILITY | PMFMHD_RAD_ROBUST_FALLBACK | PMFMHD_RAD_GLOBAL_FALLBACK))
+                PMFMHD_RAD_CHECK_ADMISSIBILITY | PMFMHD_RAD_ROBUST_FALLBACK | PMFMHD_RAD_GLOBAL_FALLBACK |
+                PMFMHD_RAD_MASKED_FALLBACK))
     return PMFMHD_EINVAL;
   if (!std::isfinite(dt) || !std::isfinite(drag_impulse) || !(drag_impulse >= 0.0f)) return PMFMHD_EINVAL;
   const bool ct = ct_packed != nullptr;
+  // the masked fallback exists in the cube kernel only, which runs GLM states
+  if (ct && (flags & PMFMHD_RAD_MASKED_FALLBACK)) return PMFMHD_EUNSUPPORTED;
   if (!ct && (!std::isfinite(ch) || !std::isfinite(decay) || !(ch > 0.0f))) return PMFMHD_EINVAL;
   // fallback steps swap the scheme without touching the caller's recon/riemann choice
   // (integrator_ref.jl:243-246, integrator_cube.jl:524-529)
@@ -535,6 +541,28 @@ int pmfmhd_step_radiation(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* cons
   // integrator_cube.jl:524-529: the global fallback launches with CHECK == 3, piecewise-constant
   // states and the admissibility test (with the robust solver if both are asked for)
   if (flags & PMFMHD_RAD_GLOBAL_FALLBACK) rf |= RAD_CHECK | RAD_FIRST_ORDER;
+  // integrator_cube.jl:527: without the global fallback, `fallback` launches with CHECK == 2, the
+  // per-cell mask in slot 4 of the correction buffer and the admissibility test
+  const float* mask = nullptr;
+  if ((flags & PMFMHD_RAD_MASKED_FALLBACK) && !(flags & PMFMHD_RAD_GLOBAL_FALLBACK)) {
+    rf |= RAD_CHECK | RAD_MASKED;
+    const long long nc = ncells(g);
+    mask = correction + 4 * nc;
+    if (flags & PMFMHD_RAD_TRACK_DENSITY) {
+      // the density increments are accumulated into that slot by this launch: read the mask
+      // from a copy taken before it
+      std::lock_guard<std::mutex> lk(c->mu);
+      if (c->mask_cells < nc) {
+        cudaFree(c->d_mask);
+        c->d_mask = nullptr;
+        c->mask_cells = 0;
+        PMF_CK(cudaMalloc(&c->d_mask, sizeof(float) * nc));
+        c->mask_cells = nc;
+      }
+      PMF_CK(cudaMemcpyAsync(c->d_mask, mask, sizeof(float) * nc, cudaMemcpyDeviceToDevice, as_stream(stream)));
+      mask = c->d_mask;
+    }
+  }
   // psi is read from slot 0 of the correction buffer, as the reference passes the buffer in
   // place of U[9]
   const float* Uin[9];
@@ -545,6 +573,7 @@ int pmfmhd_step_radiation(pmfmhd_ctx* c, const pmfmhd_grid* g, const float* cons
   st.drag = drag_coefficients(drag_impulse, nullptr);
   st.corr = correction;
   st.rad_flags = rf;
+  st.mask = mask;
   if (ct)
     return enqueue_ct(c, &g2, Uin, Unew, ct_packed, dt, nullptr, false, (rf & RAD_TRACK_MAGNETIC) != 0,
                       as_stream(stream), &st);

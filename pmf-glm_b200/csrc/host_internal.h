@@ -90,6 +90,8 @@ struct pmfmhd_ctx {
   unsigned int* d_status = nullptr;                // device status bits of the step kernels
   pmf::host::HostPath hp;                          // host-buffer step workspace
   int tma_stall_polls = 0;                         // pmfmhd_set_tma_stall test hook
+  float* d_mask = nullptr;                         // copy of a radiation fallback mask (masked step
+  long long mask_cells = 0;                        // with density tracking), allocated on first use
   std::mutex mu;
 };
 

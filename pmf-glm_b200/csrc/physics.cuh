@@ -392,9 +392,11 @@ __device__ __forceinline__ F9 hlld_x(const F9& L, const F9& R, float g, float bn
 // the selected solver (HLLD with the LLF fallback at low density/pressure), rotate back.
 // ich = 1/ch, formed once per launch: the cleaned normal field every solve starts from then
 // waits on a multiply, not on a division.
+// force_llf: LLF on this face whatever the solver (the masked fallback of the cube kernel,
+// integrator_cube.jl:68-83); false except in the radiation-coupled step.
 template <int D, int RSOL>
 __device__ __forceinline__ F9 riemann_glm(const F9& Lq, const F9& Rq, float ch, float ich, const Phys& P,
-                                          HlldCensus* cen = nullptr) {
+                                          HlldCensus* cen = nullptr, bool force_llf = false) {
   F9 L = rot_to<D>(Lq), R = rot_to<D>(Rq);
   L[0] = fmaxf(L[0], P.smallr); L[4] = fmaxf(L[4], P.pfl);
   R[0] = fmaxf(R[0], P.smallr); R[4] = fmaxf(R[4], P.pfl);
@@ -406,9 +408,10 @@ __device__ __forceinline__ F9 riemann_glm(const F9& Lq, const F9& Rq, float ch, 
   if constexpr (RSOL == RS_LLF) {
     f = llf_x(L, R, P.gamma, ch, fbn, fpsi);
   } else if constexpr (RSOL == RS_HLL) {
-    f = hll_x(L, R, P.gamma, bns, fbn, fpsi);
+    if (force_llf) f = llf_x(L, R, P.gamma, ch, fbn, fpsi);
+    else f = hll_x(L, R, P.gamma, bns, fbn, fpsi);
   } else {
-    bool uself = (P.llf_dmin > 0.0f && fminf(L[0], R[0]) < P.llf_dmin) ||
+    bool uself = force_llf || (P.llf_dmin > 0.0f && fminf(L[0], R[0]) < P.llf_dmin) ||
                  (P.llf_pmin > 0.0f && fminf(L[4], R[4]) < P.llf_pmin);
     if (uself) f = llf_x(L, R, P.gamma, ch, fbn, fpsi);
     else f = hlld_x(L, R, P.gamma, bns, fbn, fpsi, P.dtol_rel, cen);
@@ -419,7 +422,8 @@ __device__ __forceinline__ F9 riemann_glm(const F9& Lq, const F9& Rq, float ch, 
 // Constrained-transport Riemann problem (glm_physics.jl:336-348): the caller has put the
 // staggered face value into both states' normal-B slot; no psi, ch = 0 in the LLF speed.
 template <int D, int RSOL>
-__device__ __forceinline__ F9 riemann_ct(const F9& Lq, const F9& Rq, const Phys& P, HlldCensus* cen = nullptr) {
+__device__ __forceinline__ F9 riemann_ct(const F9& Lq, const F9& Rq, const Phys& P, HlldCensus* cen = nullptr,
+                                         bool force_llf = false) {
   F9 L = rot_to<D>(Lq), R = rot_to<D>(Rq);
   L[0] = fmaxf(L[0], P.smallr); L[4] = fmaxf(L[4], P.pfl); L[8] = 0.0f;
   R[0] = fmaxf(R[0], P.smallr); R[4] = fmaxf(R[4], P.pfl); R[5] = L[5]; R[8] = 0.0f;
@@ -428,9 +432,10 @@ __device__ __forceinline__ F9 riemann_ct(const F9& Lq, const F9& Rq, const Phys&
   if constexpr (RSOL == RS_LLF) {
     f = llf_x(L, R, P.gamma, 0.0f, 0.0f, 0.0f);
   } else if constexpr (RSOL == RS_HLL) {
-    f = hll_x(L, R, P.gamma, bns, 0.0f, 0.0f);
+    if (force_llf) f = llf_x(L, R, P.gamma, 0.0f, 0.0f, 0.0f);
+    else f = hll_x(L, R, P.gamma, bns, 0.0f, 0.0f);
   } else {
-    bool uself = (P.llf_dmin > 0.0f && fminf(L[0], R[0]) < P.llf_dmin) ||
+    bool uself = force_llf || (P.llf_dmin > 0.0f && fminf(L[0], R[0]) < P.llf_dmin) ||
                  (P.llf_pmin > 0.0f && fminf(L[4], R[4]) < P.llf_pmin);
     if (uself) f = llf_x(L, R, P.gamma, 0.0f, 0.0f, 0.0f);
     else f = hlld_x(L, R, P.gamma, bns, 0.0f, 0.0f, P.dtol_rel, cen);
@@ -442,10 +447,10 @@ __device__ __forceinline__ F9 riemann_ct(const F9& Lq, const F9& Rq, const Phys&
 // counted, nullptr otherwise.
 template <int D, int RSOL, bool CT>
 __device__ __forceinline__ F9 riemann(const F9& L, const F9& R, float ch, float ich, const Phys& P,
-                                      HlldCensus* cen = nullptr) {
+                                      HlldCensus* cen = nullptr, bool force_llf = false) {
   if constexpr (RSOL != RS_HLLD_CENSUS) cen = nullptr;
-  if constexpr (CT) return riemann_ct<D, RSOL>(L, R, P, cen);
-  else return riemann_glm<D, RSOL>(L, R, ch, ich, P, cen);
+  if constexpr (CT) return riemann_ct<D, RSOL>(L, R, P, cen, force_llf);
+  else return riemann_glm<D, RSOL>(L, R, ch, ich, P, cen, force_llf);
 }
 
 // max over axes of |v_d| + c_f(B_d) of a conserved state (timestep.jl:4-14)

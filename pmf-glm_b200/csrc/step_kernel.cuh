@@ -85,6 +85,7 @@ struct StepArgs {
   float* corr;              // SRC_RAD: packed 9*nc correction buffer (slot 0 psi, 1-3 velocity
                             // corrections, 4 density increments, 5-7 B / 8 E remainders)
   int rad_flags;            // SRC_RAD: RAD_* bits
+  const float* mask;        // SRC_RAD with RAD_MASKED: per-cell fallback mask (> 0: fall back)
 };
 
 // Source terms of the step (template parameter SRC of the step kernel).
@@ -92,7 +93,11 @@ enum { SRC_NONE = 0, SRC_DRAG = 1, SRC_RAD = 2 };
 // Runtime options of the radiation-coupled step (StepArgs::rad_flags).
 // RAD_FIRST_ORDER: zero reconstruction offsets in every cell, the piecewise-constant states of
 // the cube kernel's global fallback (CHECK == 3, integrator_cube.jl:168-177).
-enum { RAD_TRACK_DENSITY = 1, RAD_TRACK_MAGNETIC = 2, RAD_TRACK_ENERGY = 4, RAD_CHECK = 8, RAD_FIRST_ORDER = 16 };
+// RAD_MASKED: the cube kernel's masked fallback (CHECK == 2, integrator_cube.jl:68-83,168-171):
+// cells whose StepArgs::mask entry is positive take zero offsets, and every face with such a
+// cell on either side is solved by LLF.
+enum { RAD_TRACK_DENSITY = 1, RAD_TRACK_MAGNETIC = 2, RAD_TRACK_ENERGY = 4, RAD_CHECK = 8, RAD_FIRST_ORDER = 16,
+       RAD_MASKED = 32 };
 
 template <int TY>
 struct StepSmem {
@@ -355,6 +360,11 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   // radiation: in-plane offset of this thread's cell, wrapped periodically (halo cells and
   // the columns/rows of a partial tile beyond the grid are periodic images)
   const int rad_xy = RAD ? (((y % ny) + ny) % ny) * nx + ((x % nx) + nx) % nx : 0;
+  // masked fallback: the in-plane offsets of the cells on the lower x and y sides of this
+  // cell's lower faces (periodic images), and the mask of this cell in the previous plane
+  const bool masked = RAD && (a.rad_flags & RAD_MASKED) != 0;
+  const int rad_xm = RAD ? (((y % ny) + ny) % ny) * nx + (((x - 1) % nx) + nx) % nx : 0;
+  const int rad_ym = RAD ? ((((y - 1) % ny) + ny) % ny) * nx + ((x % nx) + nx) % nx : 0;
 
   // Where the register budget allows (TY = 8, 9: three warps per sub-partition), the state and
   // Kahan remainders of the next plane this thread updates are loaded one pass ahead, so their
@@ -441,6 +451,9 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   auto face_bn = [&](int D, int pz) {
     return __ldg(a.face[D] + wrap1(pz, nz) * nxy + wrap1(y, ny) * nx + wrap1(x, nx));
   };
+  // fallback mask of in-plane offset xy in plane pz (periodic: pz is at most one period out)
+  auto mask_at = [&](int pz, int xy) { return __ldg(a.mask + (size_t)wrap1(pz, nz) * nxy + xy) > 0.0f; };
+  bool m_zlo = false;  // mask of this cell in plane p-1 (the lower side of its z-face)
 
   F9 Fx;  // this thread's lower x-face flux of the last owned plane solved
   for (int p = z0 - 1; p <= z1; ++p) {
@@ -464,6 +477,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     F9 mh;
     Offsets<RECON> ox, oy, oz;
     float bnx = 0.0f, bny = 0.0f, bnz = 0.0f;
+    bool m_c = false;  // masked fallback: this cell of plane p is masked
     // planes z0-1 and z1 only feed the chunk's end z-faces: only the owned rows work on them
     if (mid || row_own) {
 
@@ -489,7 +503,9 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     if constexpr (RAD) {
       // piecewise-constant states: every offset replaced by zero (m0 + 0 == m0, so every face
       // state and Hancock flux difference is that of zero offsets), without a branch
-      const bool keep = (a.rad_flags & RAD_FIRST_ORDER) == 0;
+      // (all cells under the global fallback, masked cells under the masked one)
+      m_c = masked && mask_at(p, rad_xy);
+      const bool keep = (a.rad_flags & RAD_FIRST_ORDER) == 0 && !m_c;
       keep_offsets(ox, keep);
       keep_offsets(oy, keep);
       keep_offsets(oz, keep);
@@ -530,6 +546,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     }
     if (p == z0 - 1) {
       zc_store(0, face_hi<RECON>(mh, oz));
+      m_zlo = m_c;
     } else {
     if (mid && !halo_warp) {
       // upper y state for the row above (row warps 0..TY); lower y state parked (rows 1..TY+1)
@@ -562,7 +579,8 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       if constexpr (CT) {
         L[7] = bnz; R[7] = bnz;
       }
-      const F9 Fz = riemann<2, RSOL, CT>(L, R, ch, ich, P, (own && mid) ? &cz : nullptr);
+      const F9 Fz = riemann<2, RSOL, CT>(L, R, ch, ich, P, (own && mid) ? &cz : nullptr, m_zlo || m_c);
+      m_zlo = m_c;
       if constexpr (CT) {
         if (own && mid) {
           a.work[2][cell_p] = Fz[0];
@@ -614,7 +632,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
         if constexpr (CT) {
           L[5] = bnx; R[5] = bnx;
         }
-        Fx = riemann<0, RSOL, CT>(L, R, ch, ich, P, own ? &cz : nullptr);
+        Fx = riemann<0, RSOL, CT>(L, R, ch, ich, P, own ? &cz : nullptr, masked && (m_c || mask_at(p, rad_xm)));
         if (halo_warp) {
 #pragma unroll
           for (int i = 0; i < 9; ++i) fxright[hrow * 9 + i] = Fx[i];
@@ -639,7 +657,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       if constexpr (CT) {
         L[6] = bny; R[6] = bny;
       }
-      const F9 Fy = riemann<1, RSOL, CT>(L, R, ch, ich, P, own ? &cz : nullptr);
+      const F9 Fy = riemann<1, RSOL, CT>(L, R, ch, ich, P, own ? &cz : nullptr, masked && (m_c || mask_at(p, rad_ym)));
 #pragma unroll
       for (int i = 0; i < 9; ++i) fybuf[((w - 1) * 9 + i) * 32 + lane] = Fy[i];
       if constexpr (CT) {

@@ -107,8 +107,39 @@ function MHDKernels.step_ref_radiation!(s::MHDKernels.MHDState{Float32}, dt::Rea
     s.U, s.scratch = s.scratch, s.U
     s
 end
-# step_cube_radiation! adds check_admissibility (bit 3) and global_fallback (bit 5) to the
-# same call; its `fallback=true` mask mode has no counterpart and stays on the KA kernel.
+# step_cube_radiation! (integrator_cube.jl:504-540; GLM states only, as in the reference): the
+# same call with check_admissibility (bit 3), global_fallback (bit 5) and the masked fallback
+# (bit 6, `fallback=true`: slot 4 of `correction` is the per-cell mask, e.g. from
+# pmf_radiation_fallback_mask!)
+function MHDKernels.step_cube_radiation!(s::MHDKernels.MHDState{Float32}, dt::Real; ch::Real, decay::Real,
+                                         drag_impulse::Real, correction, track_density::Bool=true,
+                                         track_magnetic::Bool=true, track_energy::Bool=true,
+                                         check_admissibility::Bool=false, fallback::Bool=false,
+                                         global_fallback::Bool=false, robust_fallback::Bool=false)
+    flags = Cint(track_density) | Cint(track_magnetic) << 1 | Cint(track_energy) << 2 |
+            Cint(check_admissibility) << 3 | Cint(robust_fallback) << 4 | Cint(global_fallback) << 5 |
+            Cint(fallback) << 6
+    rc = ccall((:pmfmhd_step_radiation, libpmfmhd), Cint,
+               (Ptr{Cvoid}, Ref{PmfGrid}, Ptr{CuPtr{Float32}}, Ptr{CuPtr{Float32}}, CuPtr{Float32},
+                CuPtr{Float32}, Cfloat, Cfloat, Cfloat, Cfloat, Cint, Ptr{Cvoid}),
+               _pmf(), Ref(PmfGrid(s)), _ptrs(s.U), _ptrs(s.scratch), CuPtr{Float32}(0), pointer(correction),
+               dt, ch, decay, drag_impulse, flags, _stream())
+    rc == 0 || error("pmfmhd_step_radiation: ", _pmf_err(rc))
+    CUDA.synchronize()
+    s.U, s.scratch = s.scratch, s.U
+    s
+end
+
+# The masked fallback's mask (radiation_coupling.jl:1536-1593) into `mask` (ncells Float32 on
+# the device): from the trial density, or expanded from `mask_in` as well
+function pmf_radiation_fallback_mask!(mask, s::MHDKernels.MHDState{Float32}, trial_rho; mask_in=nothing)
+    mp = mask_in === nothing ? CuPtr{Float32}(0) : pointer(mask_in)
+    rc = ccall((:pmfmhd_radiation_fallback_mask, libpmfmhd), Cint,
+               (Ptr{Cvoid}, Ref{PmfGrid}, CuPtr{Float32}, CuPtr{Float32}, CuPtr{Float32}, Ptr{Cvoid}),
+               _pmf(), Ref(PmfGrid(s)), pointer(trial_rho), mp, pointer(mask), _stream())
+    rc == 0 || error("pmfmhd_radiation_fallback_mask: ", _pmf_err(rc))
+    mask
+end
 
 # CFL reduction (timestep.jl:37-41) without the N^3 work array or a host maximum()
 function pmf_compute_dt(s::MHDKernels.MHDState{Float32}; cfl::Real=0.4)

@@ -95,6 +95,7 @@ SIGNATURES = {
     "pmfmhd_step_ct_drag": ([_VP, _GP, _P9, _P9, _VP, ctypes.c_float, ctypes.c_float, _F3P, _VP], ctypes.c_int),
     "pmfmhd_step_radiation": ([_VP, _GP, _P9, _P9, _VP, _VP, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                ctypes.c_float, ctypes.c_int, _VP], ctypes.c_int),
+    "pmfmhd_radiation_fallback_mask": ([_VP, _GP, _VP, _VP, _VP, _VP], ctypes.c_int),
     "pmfmhd_ct_install_faces": ([_VP, _GP, _P9, _VP, _VP], ctypes.c_int),
     "pmfmhd_terminal_magnetic_force": ([_VP, _GP, _P3, _P3, _VP, _VP], ctypes.c_int),
     "pmfmhd_terminal_velocity_max": ([_VP, _GP, _P9, ctypes.c_float, ctypes.c_float, ctypes.c_float,
@@ -411,7 +412,7 @@ def step_drag_godunov(s: MHDState, dt: float, drag_impulse: float, ch: float, gl
 
 
 RAD_TRACK_DENSITY, RAD_TRACK_MAGNETIC, RAD_TRACK_ENERGY = 1, 2, 4
-RAD_CHECK_ADMISSIBILITY, RAD_ROBUST_FALLBACK, RAD_GLOBAL_FALLBACK = 8, 16, 32
+RAD_CHECK_ADMISSIBILITY, RAD_ROBUST_FALLBACK, RAD_GLOBAL_FALLBACK, RAD_MASKED_FALLBACK = 8, 16, 32, 64
 
 
 def allocate_radiation_correction(s: MHDState) -> torch.Tensor:
@@ -451,18 +452,43 @@ def step_cube_radiation(s: MHDState, dt: float, ch: float, decay: float, drag_im
                         check_admissibility: bool = False, fallback: bool = False, global_fallback: bool = False,
                         robust_fallback: bool = False) -> MHDState:
     """integrator_cube.jl:504-540 (GLM states): as step_ref_radiation, plus the admissibility
-    flag (rejected cells get density -max(|rho|, max(smallr, llf_dmin))) and the global
-    fallback (piecewise-constant states with LLF, the cube kernel's CHECK == 3). The masked
-    per-face fallback (``fallback=True``) is not provided."""
+    flag (rejected cells get density -max(|rho|, max(smallr, llf_dmin))), the global
+    fallback (piecewise-constant states with LLF, the cube kernel's CHECK == 3) and the
+    masked fallback (``fallback=True``, CHECK == 2): slot 4 of ``correction`` is a per-cell
+    mask (see ``radiation_fallback_mask``); masked cells take piecewise-constant states, every
+    face touching one is solved by LLF, and the admissibility flag is on. The mask is read as
+    it is when the call is made, before this step's density increments land in the same slot.
+    ``global_fallback`` takes precedence over ``fallback``; ``robust_fallback`` with
+    ``fallback`` runs minmod PLM / HLL with the masked cells and faces as above."""
     if uses_ct(s):
         raise PMFMHDError("step_cube_radiation!: CT is implemented on the :ref integrator only "
                           "(mhd_solver=:ct states cannot use the :cube integrators)")
-    if fallback and not global_fallback and not robust_fallback:
-        raise PMFMHDError("step_cube_radiation!: the masked per-face fallback is not provided")
     flags = ((RAD_TRACK_DENSITY if track_density else 0) | (RAD_TRACK_MAGNETIC if track_magnetic else 0)
              | (RAD_TRACK_ENERGY if track_energy else 0) | (RAD_CHECK_ADMISSIBILITY if check_admissibility else 0)
-             | (RAD_ROBUST_FALLBACK if robust_fallback else 0) | (RAD_GLOBAL_FALLBACK if global_fallback else 0))
+             | (RAD_ROBUST_FALLBACK if robust_fallback else 0) | (RAD_GLOBAL_FALLBACK if global_fallback else 0)
+             | (RAD_MASKED_FALLBACK if fallback else 0))
     return _step_radiation(s, dt, ch, decay, drag_impulse, correction, flags, "step_cube_radiation!")
+
+
+def radiation_fallback_mask(s: MHDState, trial_rho: torch.Tensor, mask_in: Optional[torch.Tensor] = None,
+                            out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """The masked fallback's mask (radiation_coupling.jl:1536-1577): 1 where the trial density
+    of a cell or of one of its six periodic face neighbours is negative, or, with ``mask_in``
+    (``_radiation_expand_fallback_mask!``), where that mask is positive there as well; 0
+    elsewhere. Returns ``out`` (a new tensor if None), which must not overlap the inputs. To
+    use it in a step, write it into slot 4 of the correction buffer."""
+    nc = s.nc
+    for t, what in ((trial_rho, "trial_rho"), (mask_in, "mask_in")):
+        if t is not None and (t.numel() != nc or t.dtype != torch.float32 or not t.is_contiguous()):
+            raise PMFMHDError(f"radiation_fallback_mask: {what} must be a contiguous float32 field of ncells values")
+    if out is None:
+        out = torch.empty(nc, dtype=torch.float32, device=trial_rho.device)
+    elif out.numel() != nc or out.dtype != torch.float32 or not out.is_contiguous():
+        raise PMFMHDError("radiation_fallback_mask: out must be a contiguous float32 field of ncells values")
+    _check(lib().pmfmhd_radiation_fallback_mask(context(s.device), ctypes.byref(s.grid), trial_rho.data_ptr(),
+                                                mask_in.data_ptr() if mask_in is not None else None,
+                                                out.data_ptr(), _stream()), "radiation_fallback_mask")
+    return out
 
 
 def apply_linear_drag(s: MHDState, decay: float, target_velocity=(0.0, 0.0, 0.0),

@@ -180,11 +180,16 @@ def test_radiation_argument_errors():
         pmfmhd.step_cube_radiation(s, 1e-3, 1.0, 1.0, -1.0, corr)
     with pytest.raises(pmfmhd.PMFMHDError):
         pmfmhd.step_cube_radiation(s, 1e-3, 1.0, 1.0, 0.1, corr[:-1])
-    with pytest.raises(pmfmhd.PMFMHDError):
-        pmfmhd.step_cube_radiation(s, 1e-3, 1.0, 1.0, 0.1, corr, fallback=True)
     c = gpu_state(problems.ct_smoke_fields(n), (n, n, n), riemann="hll", mhd_solver="ct")
     with pytest.raises(pmfmhd.PMFMHDError):
         pmfmhd.step_cube_radiation(c, 1e-3, 1.0, 1.0, 0.1, pmfmhd.allocate_radiation_correction(c))
+    # the masked fallback is a cube-kernel (GLM) mode: a CT state is refused by the C ABI too
+    with pytest.raises(pmfmhd.PMFMHDError):
+        pmfmhd._step_radiation(c, 1e-3, 0.0, 1.0, 0.1, pmfmhd.allocate_radiation_correction(c),
+                               pmfmhd.RAD_MASKED_FALLBACK, "step")
+    rho = s.U[0].clone()
+    with pytest.raises(pmfmhd.PMFMHDError):  # the mask may not overwrite its own input
+        pmfmhd.radiation_fallback_mask(s, rho, out=rho)
     o = gpu_state(problems.smooth_fields(n), (n, n, n), bcs=("outflow", "periodic", "periodic"))
     with pytest.raises(pmfmhd.PMFMHDError):
         pmfmhd.step_ref_radiation(o, 1e-3, 1.0, 1.0, 0.1, pmfmhd.allocate_radiation_correction(o))
@@ -255,3 +260,97 @@ def test_guide_field_compensated_ct_known_answer():
     h = pmfmhd.fields_to_host(sc)
     bxf = sc.ct.bxf.cpu().numpy().reshape(N, N, N)
     assert np.array_equal((f32(0.5) * (bxf + np.roll(bxf, -1, axis=2))).ravel(), h[5])
+
+
+def _pocket_state():
+    """The low-density pocket of the admissibility test, with the bulk's dt."""
+    dims = (24, 12, 10)
+    U = problems.turb_field(dims, 1.0 / 24)
+    bulk = oracle.OracleState(dims, 1.0 / 24)
+    bulk.U[:] = U
+    dt, _ = bulk.compute_dt(0.4)
+    i, j, k = problems.cell_coords(dims)
+    pocket = ((i - 12) ** 2 + (j - 6) ** 2 + (k - 5) ** 2) < 9
+    U = U.astype(np.float64)
+    U[0, pocket] *= 1e-3
+    U[1:4, pocket] *= 1e-3
+    return dims, U.astype(f32), dt
+
+
+@pytest.mark.parametrize("robust", [False, True])
+@pytest.mark.parametrize("track_density", [True, False])
+def test_masked_fallback_matches_oracle(robust, track_density):
+    """The masked fallback (fallback=true, CHECK == 2; integrator_cube.jl:68-83,168-171): the
+    mask is built from a first checked trial step as the reference's helpers would
+    (radiation_coupling.jl:1536-1577), written into slot 4, and the masked step matches the
+    oracle's — the flagged cells exactly, the others to the parity gate — in the plain
+    (HLLD) and robust (minmod PLM / HLL) schemes, with and without density tracking (which
+    accumulates into the mask's own slot)."""
+    dims, U, dt = _pocket_state()
+    nc = int(np.prod(dims))
+    # trial step, checked: rejected cells come back with negative density
+    trial = oracle.OracleState(dims, 1.0 / 24)
+    trial.U[:] = U
+    c0 = corrections(nc, 3, U[8], scale=0.0)
+    trial.step_radiation(dt, 0.1, c0, ch=1.0, decay=1.0, check_admissibility=True)
+    assert (trial.U[0] < 0).sum() > 0
+    mask_h = oracle.fallback_mask(trial.U[0], dims)
+    dev_trial = torch.from_numpy(trial.U[0].copy()).cuda()
+    dev = gpu_state(U, dims)
+    mask_d = pmfmhd.radiation_fallback_mask(dev, dev_trial)
+    assert np.array_equal(mask_d.cpu().numpy(), mask_h)
+    corr_h = corrections(nc, 3, U[8], scale=0.0)
+    corr_h[4] = mask_h
+    corr_d = torch.from_numpy(corr_h.ravel().copy()).cuda()
+    kw = dict(fallback=True, robust_fallback=robust, track_density=track_density)
+    cpu = oracle.OracleState(dims, 1.0 / 24)
+    cpu.U[:] = U
+    cpu.step_radiation(dt, 0.1, corr_h, ch=1.0, decay=1.0, **kw)
+    pmfmhd.step_cube_radiation(dev, float(dt), 1.0, 1.0, 0.1, corr_d, **kw)
+    host = pmfmhd.fields_to_host(dev)
+    flagged_cpu, flagged_dev = cpu.U[0] < 0, host[0] < 0
+    assert np.array_equal(flagged_dev, flagged_cpu)
+    ok = ~(flagged_cpu | flagged_dev)
+    assert not within_parity(cpu.U[:, ok], host[:, ok])
+    corr_parity(corr_d.cpu().numpy().reshape(9, -1), corr_h)
+
+
+def test_masked_fallback_everywhere_is_the_global_fallback_on_device():
+    """Every cell masked gives the global fallback's scheme (piecewise constant, LLF on every
+    face, admissibility flag); a mask of zeros gives the checked step. The instantiations
+    differ (HLLD with every face sent to LLF, against the LLF kernel), so the comparison is to
+    FP32 rounding, and the flags exactly."""
+    dims, U, dt = _pocket_state()
+    nc = int(np.prod(dims))
+
+    def run(mask, **kw):
+        dev = gpu_state(U, dims)
+        corr = torch.from_numpy(corrections(nc, 5, U[8], scale=0.0).ravel().copy()).cuda()
+        if mask is not None:
+            corr[4 * nc: 5 * nc] = mask
+        pmfmhd.step_cube_radiation(dev, float(dt), 1.0, 1.0, 0.1, corr, **kw)
+        return pmfmhd.fields_to_host(dev).astype(np.float64)
+
+    pairs = [(run(1.0, fallback=True), run(None, global_fallback=True)),
+             (run(0.0, fallback=True), run(None, check_admissibility=True))]
+    for a, b in pairs:
+        assert np.array_equal(a[0] < 0, b[0] < 0)
+        ok = (a[0] > 0) & (b[0] > 0)
+        for f in range(8):
+            assert np.abs(a[f, ok] - b[f, ok]).max() <= 1e-6 * np.abs(b[f]).max(), f
+
+
+def test_fallback_mask_matches_oracle():
+    """pmfmhd_radiation_fallback_mask against the numpy restatement, the first mask and the
+    expanded one, on a non-cubic periodic box."""
+    dims = (20, 12, 9)
+    nc = int(np.prod(dims))
+    rng = np.random.default_rng(11)
+    rho = np.where(rng.random(nc) < 0.03, -1.0, 1.0).astype(f32)
+    prev = (rng.random(nc) < 0.02).astype(f32)
+    s = gpu_state(np.ones((9, nc), f32), dims)  # only the grid matters here
+    r = torch.from_numpy(rho).cuda()
+    m = torch.from_numpy(prev).cuda()
+    assert np.array_equal(pmfmhd.radiation_fallback_mask(s, r).cpu().numpy(), oracle.fallback_mask(rho, dims))
+    assert np.array_equal(pmfmhd.radiation_fallback_mask(s, r, m).cpu().numpy(),
+                          oracle.fallback_mask(rho, dims, prev))
