@@ -11,7 +11,9 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("dims,bcs", [((32, 32, 32), ("periodic",) * 3), ((37, 11, 20), ("periodic",) * 3),
-                                      ((24, 16, 18), ("outflow", "periodic", "reflecting"))])
+                                      ((24, 16, 18), ("outflow", "periodic", "reflecting")),
+                                      ((32, 16, 96), ("periodic",) * 3),
+                                      ((16, 24, 70), ("periodic", "periodic", "outflow"))])
 @pytest.mark.parametrize("nchunks", [1, 3, 8])
 def test_host_step_equals_device_step(dims, bcs, nchunks):
     U = problems.turb_field(dims, 1.0 / max(dims))
