@@ -175,26 +175,48 @@ template <int RECON> __device__ __forceinline__ void keep_offsets(Offsets<RECON>
   }
 }
 
-// Half the MonCen slope, 0.5*moncen(dl, dr) of glm_physics.jl:47-53, with the scalings by
-// powers of two folded: 0.5*sgn*min(2*min|dl|,|dr|, |(dl+dr)/2|) = sgn*min(min(|dl|,|dr|),
-// |dl+dr|/4). Every rescaling is exact, so the result has the same bits.
-__device__ __forceinline__ float half_moncen(float dl, float dr) {
-  const float sum = dl + dr;
-  const float m = fminf(fminf(fabsf(dl), fabsf(dr)), 0.25f * fabsf(sum));
-  const float s = copysignf(m, sum);
-  return dl * dr <= 0.0f ? 0.0f : s;
+// min(|a|, |b|) carrying the sign sign(a) XOR sign(b) (PTX min.xorsign.abs, one instruction).
+__device__ __forceinline__ float min_xorsign_abs(float a, float b) {
+  float r;
+  asm("min.xorsign.abs.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+  return r;
+}
+// Half the MonCen slope, 0.5*moncen(dl, dr) of glm_physics.jl:47-53, from dl, dr and
+// q = (dl+dr)/4. With the scalings by powers of two folded, the reference's value is
+// 0.5*sgn*min(2*min|dl|,|dr|, |(dl+dr)/2|) = sgn(q)*min(min(|dl|,|dr|), |q|) when dl*dr > 0 and
+// 0 otherwise. t = min.xorsign.abs(dl, dr) has magnitude min(|dl|,|dr|) and is positive exactly
+// when dl and dr have the same sign, so max(t, 0) is zero wherever the reference returns zero,
+// and min.xorsign.abs(max(t, 0), q) carries sgn(q): three instructions, the same value (up to
+// the sign of a zero result), every step exact.
+__device__ __forceinline__ float half_moncen(float dl, float dr, float q) {
+  return min_xorsign_abs(fmaxf(min_xorsign_abs(dl, dr), 0.0f), q);
+}
+// Two fields at once: the differences and the quarter sum as packed pairs (each lane rounded as
+// the scalar operation), the limiter per lane.
+__device__ __forceinline__ float2 half_moncen2(float2 mm, float2 m0, float2 mp) {
+  const float2 dl = sub2(m0, mm), dr = sub2(mp, m0);
+  const float2 q = mul2(pb(0.25f), add2(dl, dr));
+  return make_float2(half_moncen(dl.x, dr.x, q.x), half_moncen(dl.y, dr.y, q.y));
 }
 
 template <int RECON>
 __device__ __forceinline__ Offsets<RECON> recon(const F9& mm, const F9& m0, const F9& mp) {
   Offsets<RECON> o;
+  if constexpr (RECON == RECON_PLM) {
 #pragma unroll
-  for (int i = 0; i < 9; ++i) {
-    if constexpr (RECON == RECON_PLM) {
-      o.dR[i] = half_moncen(m0[i] - mm[i], mp[i] - m0[i]);
-    } else if constexpr (RECON == RECON_PLM_MINMOD) {
-      o.dR[i] = 0.5f * minmod(m0[i] - mm[i], mp[i] - m0[i]);
-    } else {
+    for (int i = 0; i < 8; i += 2) {
+      const float2 h = half_moncen2(p2(mm[i], mm[i + 1]), p2(m0[i], m0[i + 1]), p2(mp[i], mp[i + 1]));
+      o.dR[i] = h.x;
+      o.dR[i + 1] = h.y;
+    }
+    const float dl = m0[8] - mm[8], dr = mp[8] - m0[8];
+    o.dR[8] = half_moncen(dl, dr, 0.25f * (dl + dr));
+  } else if constexpr (RECON == RECON_PLM_MINMOD) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) o.dR[i] = 0.5f * minmod(m0[i] - mm[i], mp[i] - m0[i]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
       float a, b;
       ppm_edges(mm[i], m0[i], mp[i], a, b);
       o.dL[i] = a - m0[i];
@@ -241,7 +263,8 @@ __device__ __forceinline__ P9 phys_flux_x2(const P9& q, float g) {
 }
 
 // flux difference F(m0 + dR) - F(m0 + dL) along axis D (one term of the Hancock predictor,
-// glm_physics.jl:225-231); the two face states are evaluated as one packed pair
+// glm_physics.jl:225-231); the flux of the two face states is evaluated as one packed pair (the
+// states themselves are formed by scalar adds, which write the pair's registers directly)
 template <int D, int RECON>
 __device__ __forceinline__ F9 hancock_term(const F9& m0, const Offsets<RECON>& o, float g) {
   // global -> D-normal component order, as rot_to<D>
@@ -250,7 +273,7 @@ __device__ __forceinline__ F9 hancock_term(const F9& m0, const Offsets<RECON>& o
 #pragma unroll
   for (int i = 0; i < 9; ++i) {
     const int j = perm[D][i];
-    q[i] = add2(pb(m0[j]), p2(o.dR[j], o.l(j)));
+    q[i] = make_float2(m0[j] + o.dR[j], m0[j] + o.l(j));
   }
   const P9 f = phys_flux_x2(q, g);
   F9 d;

@@ -14,13 +14,16 @@
 //     state from lane l-1 by __shfl_up (lane 0 takes the left halo cell's state from shared
 //     memory); the face above lane 31 is solved by the halo warp.
 //   * y-faces exchange one 9-float state per thread through shared memory.
-//   * z-faces never leave registers: each thread keeps the upper z-face state, the lower
-//     z-face flux and the x/y flux divergence of the previous plane of its own column, so
-//     plane p-1 is updated as soon as the z-face p-1/2 is solved in the pass over plane p.
-// Primitives of planes p-1, p, p+1 (with a 2-cell ring) live in a 3-slot shared ring; the
-// raw conserved plane p+2 is prefetched into a staging buffer by cp.async while plane p is
-// computed. Each face is solved exactly once per CTA; the only recomputation is the Hancock
-// state of the one-cell halo ring and the halo rows' y-faces.
+//   * z-faces never leave the column: each thread keeps the upper z-face state, the lower
+//     z-face flux and the x/y flux divergence of the previous plane of its own column (in
+//     private shared-memory slots), so plane p-1 is updated as soon as the z-face p-1/2 is
+//     solved in the pass over plane p.
+// Primitives of planes p-1, p, p+1 (with a 2-cell ring) live in a 4-slot shared ring, into
+// which three loader warps convert plane p+2 while plane p is computed; the raw conserved
+// planes come in by TMA (interior columns) or cp.async (boundary columns). Every 9-field
+// vector in shared memory is stored in float4 blocks (three instructions per vector). Each
+// face is solved exactly once per CTA; the only recomputation is the Hancock state of the
+// one-cell halo ring and the halo rows' y-faces.
 // The new state's max signal speed (timestep.jl:4-14) is reduced in the same pass.
 #pragma once
 #include <cuda.h>  // CUtensorMap (the tiled-tensor descriptor the TMA loads read)
@@ -103,20 +106,50 @@ template <int TY>
 struct StepSmem {
   static constexpr int PH = TY + 4;                 // rows y0-2 .. y0+TY+1
   static constexpr int PW = PLANE_W * PH;           // cells per staged plane
-  static constexpr int PP = (PW + 31) / 32 * 32;    // field stride: 128-byte aligned for TMA
-  static constexpr int STAGE = 9 * PP;              // raw conserved plane
+  static constexpr int PP = (PW + 31) / 32 * 32;    // staging field stride: 128-byte aligned for TMA
+  static constexpr int STAGE = 9 * PP;              // raw conserved plane, [field][cell]
   static constexpr int NSTAGE = step_double_stage<TY>() ? 2 : 1;  // staging buffers
-  static constexpr int PRIM = 4 * 9 * PP;           // 4-plane primitive ring
-  static constexpr int YB = (TY + 1) * 9 * 32;      // y-face states / fluxes
+  // Primitive planes in blocks (fields 0-3 and 4-7 as one float4 per cell, field 8 as a float),
+  // so a cell's nine values move in three shared-memory instructions. Rows are PRW = 42 cells
+  // apart: the halo warp's lanes, which read two columns of eight rows, then hit distinct banks.
+  static constexpr int PRW = 42;
+  static constexpr int PPC = (PH * PRW + 3) / 4 * 4;  // cells per primitive plane (16-byte blocks)
+  static constexpr int PRIM = 4 * 9 * PPC;          // 4-plane primitive ring
+  static constexpr int G9 = 9 * 32;                 // one 9-vector per lane, in the same blocks
+  static constexpr int YB = (TY + 1) * G9;          // y-face states / fluxes
+  static constexpr int ZC = TY * 3 * G9;            // per owned thread: upper z state, lower z flux, x/y divergence
+  static constexpr int YL = (TY + 1) * G9;          // lower y state of rows 1..TY+1, parked
   static constexpr int XB = TY * 9;                 // one x-face state or flux per owned row
-  static constexpr int ZC = TY * 27 * 32;           // per owned thread: upper z state, lower z flux, x/y divergence
-  static constexpr int YL = (TY + 1) * 9 * 32;      // lower y state of rows 1..TY+1, parked
   static constexpr int NL = 96;                     // loader threads: warps 0, TY+1 and the halo warp
   static constexpr int KL = (PW + NL - 1) / NL;     // staged entries per loader thread
-  static constexpr int SI = 2 * KL * NL;            // per loader: source (x, y) offset and flip bits
-  static constexpr int FLOATS = NSTAGE * STAGE + PRIM + 2 * YB + 3 * XB + ZC + YL + SI;
+  static constexpr int SI = 2 * KL * NL;            // per loader: source (x, y) offset; ring cell and flip bits
+  static constexpr int FLOATS = NSTAGE * STAGE + PRIM + 2 * YB + ZC + YL + 3 * XB + SI;
   static constexpr size_t BYTES = sizeof(float) * FLOATS;
 };
+
+// Nine floats of one lane in a block group g of G9 floats: fields 0-3 at float4 [lane], fields
+// 4-7 at float4 [32 + lane], field 8 at float [256 + lane]; every access is conflict-free.
+__device__ __forceinline__ void st9g(float* g, int lane, const F9& v) {
+  reinterpret_cast<float4*>(g)[lane] = make_float4(v[0], v[1], v[2], v[3]);
+  reinterpret_cast<float4*>(g)[32 + lane] = make_float4(v[4], v[5], v[6], v[7]);
+  g[256 + lane] = v[8];
+}
+__device__ __forceinline__ F9 ld9g(const float* g, int lane) {
+  const float4 a = reinterpret_cast<const float4*>(g)[lane];
+  const float4 b = reinterpret_cast<const float4*>(g)[32 + lane];
+  return F9{{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, g[256 + lane]}};
+}
+// Nine fields of cell c of a primitive plane of NC cells (blocks of NC float4, NC float4, NC floats).
+template <int NC> __device__ __forceinline__ void st9p(float* pl, int c, const F9& v) {
+  reinterpret_cast<float4*>(pl)[c] = make_float4(v[0], v[1], v[2], v[3]);
+  reinterpret_cast<float4*>(pl)[NC + c] = make_float4(v[4], v[5], v[6], v[7]);
+  pl[8 * NC + c] = v[8];
+}
+template <int NC> __device__ __forceinline__ F9 ld9p(const float* pl, int c) {
+  const float4 a = reinterpret_cast<const float4*>(pl)[c];
+  const float4 b = reinterpret_cast<const float4*>(pl)[NC + c];
+  return F9{{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, pl[8 * NC + c]}};
+}
 
 __device__ __forceinline__ void cp_async4(float* smem_dst, const float* gsrc) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
@@ -142,14 +175,15 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   float* prim = smem + S::NSTAGE * S::STAGE;
   // the staging buffer of plane zp (zp >= z0 - 2 >= -2)
   auto stage_of = [&](int zp) { return DSTAGE ? stage + ((zp + 4) & 1) * S::STAGE : stage; };
-  float* ybuf = prim + S::PRIM;
-  float* fybuf = ybuf + S::YB;
-  float* xleft = fybuf + S::YB;    // [row][9] upper x state of the left halo cell
+  // 9-vector groups (st9g / ld9g), 16-byte aligned: every size before them is a multiple of 4
+  float* ybuf = prim + S::PRIM;    // [row] upper y state of rows 0..TY
+  float* fybuf = ybuf + S::YB;     // [row-1] flux through the lower y face of rows 1..TY+1
+  float* zcarry = fybuf + S::YB;   // [row][3] upper z state, lower z flux, x/y divergence of p-1
+  float* ylow = zcarry + S::ZC;    // [row-1] lower y state of rows 1..TY+1
+  float* xleft = ylow + S::YL;     // [row][9] upper x state of the left halo cell
   float* xright = xleft + S::XB;   // [row][9] upper x state of lane 31
   float* fxright = xright + S::XB; // [row][9] flux through the face above lane 31
-  float* zcarry = fxright + S::XB; // [row][27][32] upper z state, lower z flux, x/y divergence of p-1
-  float* ylow = zcarry + S::ZC;    // [row-1][9][32] lower y state of rows 1..TY+1
-  int* sidx = reinterpret_cast<int*>(ylow + S::YL);  // [KL][2][NL] staging map of this segment
+  int* sidx = reinterpret_cast<int*>(fxright + S::XB);  // [KL][2][NL] staging map of this segment
 
   const int tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5;
@@ -179,9 +213,10 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   const bool loader = w == 0 || w >= TY + 1;
   const int lt = w == 0 ? lane : (w == TY + 1 ? 32 + lane : 64 + lane);
   // Staging map of this column: for each staged entry e (row r, column c) a loader handles,
-  // the in-plane source offset iy*nx+ix under the x/y boundary rules and the reflecting-wall
-  // flips (bit 0: x, bit 1: y). It is the same for every plane, so it is built once per
-  // segment; per plane only the z index is resolved.
+  // the in-plane source offset iy*nx+ix under the x/y boundary rules, and the entry's cell in
+  // the primitive ring (bits 2..) with the reflecting-wall flips (bit 0: x, bit 1: y). It is
+  // the same for every plane, so it is built once per segment; per plane only the z index is
+  // resolved.
   if (loader) {
 #pragma unroll
     for (int k = 0; k < S::KL; ++k) {
@@ -192,7 +227,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
         const int ix = bc_index(x0 + c - PLANE_X0, nx, a.bc[0], &fx);
         const int iy = bc_index(y0 + r - 2, ny, a.bc[1], &fy);
         sidx[(2 * k) * S::NL + lt] = iy * nx + ix;
-        sidx[(2 * k + 1) * S::NL + lt] = (fx < 0.0f ? 1 : 0) | (fy < 0.0f ? 2 : 0);
+        sidx[(2 * k + 1) * S::NL + lt] = ((r * S::PRW + c) << 2) | (fx < 0.0f ? 1 : 0) | (fy < 0.0f ? 2 : 0);
       }
     }
   }
@@ -295,9 +330,7 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
           u[2] *= fy; u[6] *= fy;
           u[3] *= fz; u[7] *= fz;
         }
-        F9 q = cons2prim(u, g, P.smallr, P.pfl);
-#pragma unroll
-        for (int f = 0; f < 9; ++f) dst[f * PP + e] = q[f];
+        st9p<S::PPC>(dst, fl >> 2, cons2prim(u, g, P.smallr, P.pfl));
       }
     }
   };
@@ -307,13 +340,8 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   };
   // barrier among the loader warps only (named barrier 1)
   auto loader_sync = [&]() { asm volatile("bar.sync 1, %0;\n" ::"r"(S::NL) : "memory"); };
-  auto slot = [&](int zp) { return prim + ((zp - z0 + 4) & 3) * (9 * PP); };
-  auto ld9 = [&](const float* pl, int r, int c) {
-    F9 q;
-#pragma unroll
-    for (int f = 0; f < 9; ++f) q[f] = pl[f * PP + r * PLANE_W + c];
-    return q;
-  };
+  auto slot = [&](int zp) { return prim + ((zp - z0 + 4) & 3) * (9 * S::PPC); };
+  auto ld9 = [&](const float* pl, int r, int c) { return ld9p<S::PPC>(pl, r * S::PRW + c); };
 
   // Prologue: primitives of planes z0-2, z0-1 and z0, plane z0+1 in flight.
   __syncthreads();  // the previous segment may still be reading shared memory
@@ -339,20 +367,13 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   }
 
   // Per-column carries across planes (owned rows only), in this thread's private slots of
-  // `zcarry`: the upper z-face state (0..8) and the lower z-face flux (9..17) of plane p-1 and
-  // its x/y divergence ((Fxl - Fxh) + (Fyl - Fyh), 18..26). Parking them in shared memory
+  // `zcarry`: the upper z-face state (ZC_STATE) and the lower z-face flux (ZC_FLUX) of plane p-1
+  // and its x/y divergence ((Fxl - Fxh) + (Fyl - Fyh), ZC_DIV). Parking them in shared memory
   // keeps only the current solve's states in registers.
-  float* zc = zcarry + (row_own ? (w - 1) : 0) * 27 * 32 + lane;
-  auto zc_store = [&](int off, const F9& v) {
-#pragma unroll
-    for (int i = 0; i < 9; ++i) zc[(off + i) * 32] = v[i];
-  };
-  auto zc_load = [&](int off) {
-    F9 v;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) v[i] = zc[(off + i) * 32];
-    return v;
-  };
+  enum { ZC_STATE = 0, ZC_FLUX = 1, ZC_DIV = 2 };
+  float* zc = zcarry + (row_own ? (w - 1) : 0) * 3 * S::G9;
+  auto zc_store = [&](int k, const F9& v) { st9g(zc + k * S::G9, lane, v); };
+  auto zc_load = [&](int k) { return ld9g(zc + k * S::G9, lane); };
   // this thread's cell in the staged plane (halo lanes beyond 2*TY read a valid dummy cell)
   const int r0 = halo_warp ? (halo_act ? hrow + 2 : 2) : w + 1;
   const int c0 = halo_warp ? (hside ? PLANE_X0 + TILE_X : PLANE_X0 - 1) : PLANE_X0 + lane;
@@ -463,13 +484,14 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     // of this pass (the face above lane 31 comes from the halo warp)
     if (row_own && p > z0) {
       F9 dxy;
+      const F9 fyl = ld9g(fybuf + (w - 1) * S::G9, lane), fyh = ld9g(fybuf + w * S::G9, lane);
 #pragma unroll
       for (int i = 0; i < 9; ++i) {
         const float dn = __shfl_down_sync(0xffffffffu, Fx[i], 1);
         const float fxh = lane == TILE_X - 1 ? fxright[(w - 1) * 9 + i] : dn;
-        dxy[i] = (Fx[i] - fxh) + (fybuf[((w - 1) * 9 + i) * 32 + lane] - fybuf[(w * 9 + i) * 32 + lane]);
+        dxy[i] = (Fx[i] - fxh) + (fyl[i] - fyh[i]);
       }
-      zc_store(18, dxy);
+      zc_store(ZC_DIV, dxy);
     }
     const bool mid = p >= z0 && p < z1;  // an owned plane of this chunk
     const int cell_p = (mid && x < nx && y < ny) ? (p * nxy + y * nx + x) : 0;
@@ -545,21 +567,13 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
       }
     }
     if (p == z0 - 1) {
-      zc_store(0, face_hi<RECON>(mh, oz));
+      zc_store(ZC_STATE, face_hi<RECON>(mh, oz));
       m_zlo = m_c;
     } else {
     if (mid && !halo_warp) {
       // upper y state for the row above (row warps 0..TY); lower y state parked (rows 1..TY+1)
-      if (w <= TY) {
-        const F9 yR = face_hi<RECON>(mh, oy);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) ybuf[(w * 9 + i) * 32 + lane] = yR[i];
-      }
-      if (w >= 1) {
-        const F9 yL = face_lo<RECON>(mh, oy);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) ylow[((w - 1) * 9 + i) * 32 + lane] = yL[i];
-      }
+      if (w <= TY) st9g(ybuf + w * S::G9, lane, face_hi<RECON>(mh, oy));
+      if (w >= 1) st9g(ylow + (w - 1) * S::G9, lane, face_lo<RECON>(mh, oy));
     }
     // x-face states at the tile edges go through shared memory
     if (mid && row_own && lane == TILE_X - 1) {
@@ -574,8 +588,8 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     }
     if (row_own) {
       // ---- z-face p-1/2: left = carried upper z state of p-1, right = lower z state of p --
-      F9 L = zc_load(0), R = face_lo<RECON>(mh, oz);
-      zc_store(0, face_hi<RECON>(mh, oz));
+      F9 L = zc_load(ZC_STATE), R = face_lo<RECON>(mh, oz);
+      zc_store(ZC_STATE, face_hi<RECON>(mh, oz));
       if constexpr (CT) {
         L[7] = bnz; R[7] = bnz;
       }
@@ -588,11 +602,11 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
           a.work[8][cell_p] = Fz[6];
         }
       }
-      if (p > z0 && own) update_cell(p - 1, zc_load(18), zc_load(9), Fz);
+      if (p > z0 && own) update_cell(p - 1, zc_load(ZC_DIV), zc_load(ZC_FLUX), Fz);
       if constexpr (PREFETCH) {
         if (mid && own) prefetch_cell(p);
       }
-      zc_store(9, Fz);
+      zc_store(ZC_FLUX, Fz);
     }
     }  // p > z0 - 1
     }  // mid || row_own
@@ -648,18 +662,12 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
     }
     // ---- y-faces: rows 1..TY+1 solve the face below them from two shared-memory states ---
     if (w >= 1 && !halo_warp) {
-      F9 L, R;
-#pragma unroll
-      for (int i = 0; i < 9; ++i) {
-        L[i] = ybuf[((w - 1) * 9 + i) * 32 + lane];
-        R[i] = ylow[((w - 1) * 9 + i) * 32 + lane];
-      }
+      F9 L = ld9g(ybuf + (w - 1) * S::G9, lane), R = ld9g(ylow + (w - 1) * S::G9, lane);
       if constexpr (CT) {
         L[6] = bny; R[6] = bny;
       }
       const F9 Fy = riemann<1, RSOL, CT>(L, R, ch, ich, P, own ? &cz : nullptr, masked && (m_c || mask_at(p, rad_ym)));
-#pragma unroll
-      for (int i = 0; i < 9; ++i) fybuf[((w - 1) * 9 + i) * 32 + lane] = Fy[i];
+      st9g(fybuf + (w - 1) * S::G9, lane, Fy);
       if constexpr (CT) {
         if (own) {
           a.work[1][cell_p] = Fy[0];
