@@ -507,25 +507,27 @@ def big_box_cases():
     return out
 
 
-def plain_port(s, U_host, dt, sp, decay, steps, warmup):
+def plain_port(s, U_host, dt, sp, decay, steps, warmup, entry="pmfport_step_glm"):
     """The plain single-instance FP32 port (pmf-glm_b200/libpmfport.so: one thread per cell,
     the reference's per-cell kernel with its seven Hancock predictions and six Riemann solves per
-    cell) on the same state and fixed dt: device ms per step."""
+    cell) on the same state and fixed dt: device ms per step. `entry` pmfport_step_glm shares the
+    library's arithmetic; pmfport_step_glm_refarith has the reference's scalar forms."""
     import ctypes
 
     import torch
 
     import pmfmhd
     L = ctypes.CDLL(os.path.join(ROOT, "pmf-glm_b200", "libpmfport.so"))
-    L.pmfport_step_glm.argtypes = [ctypes.POINTER(pmfmhd.Grid), pmfmhd._P9, pmfmhd._P9, ctypes.c_float,
-                                   ctypes.c_float, ctypes.c_float, ctypes.c_void_p]
+    fn = getattr(L, entry)
+    fn.argtypes = [ctypes.POINTER(pmfmhd.Grid), pmfmhd._P9, pmfmhd._P9, ctypes.c_float, ctypes.c_float,
+                   ctypes.c_float, ctypes.c_void_p]
     pmfmhd.set_fields(s, U_host)
 
     def one():
-        rc = L.pmfport_step_glm(ctypes.byref(s.grid), pmfmhd._p9(s.U), pmfmhd._p9(s.scratch), float(dt), float(sp),
-                                float(decay), pmfmhd._stream())
+        rc = fn(ctypes.byref(s.grid), pmfmhd._p9(s.U), pmfmhd._p9(s.scratch), float(dt), float(sp), float(decay),
+                pmfmhd._stream())
         if rc != 0:
-            raise RuntimeError(f"pmfport_step_glm: {rc}")
+            raise RuntimeError(f"{entry}: {rc}")
         s.U, s.scratch = s.scratch, s.U
     for _ in range(warmup):
         one()
@@ -801,8 +803,12 @@ def main():
         del r, hr
         # the plain single-instance FP32 port of the reference's per-cell kernel, same box
         port_ms = plain_port(s, U_host, dt, sp, decay, min(args.steps, 10), 2)
+        ref_ms = plain_port(s, U_host, dt, sp, decay, min(args.steps, 10), 2, "pmfport_step_glm_refarith")
         extra["plain_port"] = {"value": n ** 3 / (port_ms / 1e3), "ms_per_step": port_ms,
-                               "fused_speedup": port_ms / kernel_ms}
+                               "fused_speedup": port_ms / kernel_ms,
+                               "arithmetic": "the library's (decomposition-only comparison)",
+                               "reference_arithmetic": {"value": n ** 3 / (ref_ms / 1e3), "ms_per_step": ref_ms,
+                                                        "fused_speedup": ref_ms / kernel_ms}}
         # CT side by side on the same generator (faces from the edge potential)
         boxc = ics.turbulent_box(n, seed=0, with_ct=True)
         c = pmfmhd.set_fields(pmfmhd.allocate_state((n, n, n), 1.0 / n, mhd_solver="ct"), boxc["U"])
@@ -838,6 +844,7 @@ def main():
         cm = a0.elapsed_time(a1) / args.steps
         extra["compensated"] = {"value": n ** 3 / (cm / 1e3), "ms_per_step": cm}
         extra["plain_port"]["compensated_speedup"] = extra["plain_port"]["ms_per_step"] / cm
+        extra["plain_port"]["reference_arithmetic"]["compensated_speedup"] = ref_ms / cm
         del q
         if world == 1:
             extra["batched"] = batched_mix()

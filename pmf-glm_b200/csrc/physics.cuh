@@ -130,13 +130,7 @@ template <int D> __device__ __forceinline__ F9 dir_flux(const F9& q, float g) {
   return rot_back<D>(phys_flux_x(rot_to<D>(q), g));
 }
 
-// MonCen (slope_type 2) and minmod limiters (glm_physics.jl:47-59)
-__device__ __forceinline__ float moncen(float dl, float dr) {
-  float dc = 0.5f * (dl + dr);
-  float sgn = dc >= 0.0f ? 1.0f : -1.0f;
-  float val = sgn * fminf(2.0f * fminf(fabsf(dl), fabsf(dr)), fabsf(dc));
-  return dl * dr <= 0.0f ? 0.0f : val;
-}
+// minmod limiter (glm_physics.jl:54-59); MonCen is half_moncen below
 __device__ __forceinline__ float minmod(float dl, float dr) {
   float sgn = dl >= 0.0f ? 1.0f : -1.0f;
   return dl * dr <= 0.0f ? 0.0f : sgn * fminf(fabsf(dl), fabsf(dr));
