@@ -63,7 +63,10 @@ def compensated_only(args):
                           ics.turbulent_box(n, seed=0)["U"])
     dt, sp = pmfmhd.compute_dt(s, 0.2)
     decay = float(np.exp(np.float32(np.float32(np.float32(-0.18) * np.float32(sp)) * np.float32(dt)) / np.float32(s.dx)))
-    pmfmhd.autotune(s)
+    if args.rows:
+        pmfmhd.set_tile(s, args.rows, 16)
+    else:
+        pmfmhd.autotune(s)
     for _ in range(args.warmup):
         pmfmhd.step_cube(s, dt, sp, decay)
     torch.cuda.synchronize()
