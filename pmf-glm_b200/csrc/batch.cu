@@ -307,7 +307,8 @@ int pmfmhd_batch_create(pmfmhd_ctx* c, const pmfmhd_box* boxes, int nbox, pmfmhd
         a.smax_bits = g.ct ? nullptr : b->d_smax + i;
         a.dscal = b->d_dscal + 4 * i;
         a.status = c->d_status;
-        a.use_tma = field_maps(c, &x.grid, a.U, g.ty, a.tmap) ? 1 : 0;
+        // CT boxes stage by cp.async, as the single-box CT step does
+        a.use_tma = (!g.ct && field_maps(c, &x.grid, a.U, g.ty, a.tmap)) ? 1 : 0;
         d.q0 = q;
         desc[p].push_back(d);
       }
