@@ -307,8 +307,7 @@ int pmfmhd_batch_create(pmfmhd_ctx* c, const pmfmhd_box* boxes, int nbox, pmfmhd
         a.smax_bits = g.ct ? nullptr : b->d_smax + i;
         a.dscal = b->d_dscal + 4 * i;
         a.status = c->d_status;
-        // CT boxes stage by cp.async, as the single-box CT step does
-        a.use_tma = (!g.ct && field_maps(c, &x.grid, a.U, g.ty, a.tmap)) ? 1 : 0;
+        a.use_tma = 0;  // the batched kernel stages every plane by cp.async
         d.q0 = q;
         desc[p].push_back(d);
       }

@@ -160,7 +160,8 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // One column segment: planes [z0, z1) of column tile (tx, ty) of the box described by `a`.
 // Every thread of the CTA calls it; `smax` accumulates the new state's max signal speed.
-template <int TY, int RECON, int RSOL, bool CT, bool COMP, int SRC>
+// TMA: the instantiation carries the bulk-tensor staging path (used where a.use_tma is set).
+template <int TY, int RECON, int RSOL, bool CT, bool COMP, int SRC, bool TMA>
 __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, int z0, int z1, float* smem,
                                              float& smax, unsigned long long* tma_bar, unsigned& tma_phase,
                                              int* tma_off, HlldCensus& cz) {
@@ -237,10 +238,6 @@ __device__ __forceinline__ void march_column(const StepArgs& a, int tx, int ty, 
   // staging map. After a bounded TMA wait has given up (*tma_off set), a late copy may still
   // land in `stage`, so the staging buffer is never touched again in this launch: every later
   // plane is converted straight from global memory.
-  // The CT instantiations are compiled without the TMA path (the host never enables it for
-  // them): dropping its code made the CT Godunov stage 4 % faster at 8 rows (2.29 against 2.38 ms
-  // per 256^3 step), where the same build of the GLM step gained 0.5 % and keeps TMA.
-  constexpr bool TMA = !CT;
   const bool tma_cols = TMA && a.use_tma && (__cvta_generic_to_shared(stage) & 127) == 0 && x0 - PLANE_X0 >= 0 &&
                         x0 - PLANE_X0 + PLANE_W <= nx && y0 - 2 >= 0 && y0 + TY + 2 <= ny;
   bool pending_tma = false;  // the plane in flight came by TMA
@@ -749,7 +746,10 @@ __device__ __forceinline__ void cta_range(long long Q, long long* q0, long long*
   *q1 = Q * (blockIdx.x + 1) / gridDim.x;
 }
 
-// One box: a persistent launch of one CTA per resident slot.
+// One box: a persistent launch of one CTA per resident slot. The GLM instantiations stage
+// interior planes by TMA; the CT ones are compiled without the TMA path and stage every plane by
+// cp.async: the path's code cost the CT stage 4 % at 8 rows (2.38 against 2.29 ms per 256^3
+// step), the GLM step 0.5 %.
 template <int TY, int RECON, int RSOL, bool CT, bool COMP, int SRC>
 __global__ void __launch_bounds__(step_threads<TY>(), step_min_blocks<TY>()) mhd_step_kernel(const __grid_constant__ StepArgs a) {
   extern __shared__ __align__(128) float smem[];
@@ -767,7 +767,7 @@ __global__ void __launch_bounds__(step_threads<TY>(), step_min_blocks<TY>()) mhd
     const int zr = (int)(q - (long long)col * nzr);
     const int z0 = a.zlo + zr;
     const int z1 = a.zlo + (int)min((long long)nzr, zr + (qe - q));
-    march_column<TY, RECON, RSOL, CT, COMP, SRC>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar,
+    march_column<TY, RECON, RSOL, CT, COMP, SRC, !CT>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar,
                                                   tma_phase, &tma_off, cz);
     q += z1 - z0;
   }
@@ -778,7 +778,9 @@ __global__ void __launch_bounds__(step_threads<TY>(), step_min_blocks<TY>()) mhd
 }
 
 // Many boxes in one launch: box b owns global indices [q0_b, q0_{b+1}) of the concatenated
-// (column, plane) spaces; each CTA walks its equal share across box boundaries.
+// (column, plane) spaces; each CTA walks its equal share across box boundaries. Compiled
+// without the TMA path, every plane staged by cp.async: with it the batch kernel sat at its
+// register cap (168 against 158) and one 256^3 box took 2.06 ms per step against 1.82 ms.
 struct alignas(64) BoxStep {
   StepArgs a;     // per-box pointers, extents and parameters; dscal = that box's {dt/dx, ch, decay}
   long long q0;   // first global (column, plane) index of this box
@@ -814,7 +816,7 @@ __global__ void __launch_bounds__(step_threads<TY>(), step_min_blocks<TY>()) mhd
     const int col = (int)(local / a.nz);
     const int z0 = (int)(local - (long long)col * a.nz);
     const int z1 = (int)min((long long)a.nz, z0 + (qe - q));
-    march_column<TY, RECON, RSOL, CT, COMP, SRC_NONE>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar,
+    march_column<TY, RECON, RSOL, CT, COMP, SRC_NONE, false>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar,
                                                    tma_phase, &tma_off, cz);
     q += z1 - z0;
   }
