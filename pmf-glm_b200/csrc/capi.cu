@@ -173,9 +173,10 @@ int launch_step(pmfmhd_ctx* c, const pmfmhd_grid* g, StepArgs& a, Tune t, bool c
   a.P = phys_of(g);
   a.status = c->d_status;
   a.tma_stall_polls = c->tma_stall_polls;
-  // Interior planes come in by TMA for the GLM step; the CT instantiations are compiled
-  // without the TMA path and stage every plane by per-element cp.async.
-  a.use_tma = (!ct && field_maps(c, g, a.U, t.ty, a.tmap)) ? 1 : 0;
+  // Interior planes come in by TMA for the plain and compensated GLM step; the CT and
+  // source-coupled instantiations are compiled without the TMA path and stage every plane by
+  // per-element cp.async.
+  a.use_tma = (!ct && src == SRC_NONE && field_maps(c, g, a.U, t.ty, a.tmap)) ? 1 : 0;
   if (a.zhi <= a.zlo) {  // the whole box unless the caller set a plane range
     a.zlo = 0;
     a.zhi = g->nz;

@@ -746,10 +746,10 @@ __device__ __forceinline__ void cta_range(long long Q, long long* q0, long long*
   *q1 = Q * (blockIdx.x + 1) / gridDim.x;
 }
 
-// One box: a persistent launch of one CTA per resident slot. The GLM instantiations stage
-// interior planes by TMA; the CT ones are compiled without the TMA path and stage every plane by
-// cp.async: the path's code cost the CT stage 4 % at 8 rows (2.38 against 2.29 ms per 256^3
-// step), the GLM step 0.5 %.
+// One box: a persistent launch of one CTA per resident slot. The plain and compensated GLM
+// instantiations stage interior planes by TMA; the CT and source-coupled ones are compiled
+// without the TMA path and stage every plane by cp.async: the path's code cost them 4 % (CT,
+// 2.38 against 2.29 ms per 256^3 step), 2 % (drag) and 5 % (radiation), the GLM step 0.5 %.
 template <int TY, int RECON, int RSOL, bool CT, bool COMP, int SRC>
 __global__ void __launch_bounds__(step_threads<TY>(), step_min_blocks<TY>()) mhd_step_kernel(const __grid_constant__ StepArgs a) {
   extern __shared__ __align__(128) float smem[];
@@ -767,7 +767,7 @@ __global__ void __launch_bounds__(step_threads<TY>(), step_min_blocks<TY>()) mhd
     const int zr = (int)(q - (long long)col * nzr);
     const int z0 = a.zlo + zr;
     const int z1 = a.zlo + (int)min((long long)nzr, zr + (qe - q));
-    march_column<TY, RECON, RSOL, CT, COMP, SRC, !CT>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar,
+    march_column<TY, RECON, RSOL, CT, COMP, SRC, !CT && SRC == SRC_NONE>(a, col % a.ntx, col / a.ntx, z0, z1, smem, smax, &tma_bar,
                                                   tma_phase, &tma_off, cz);
     q += z1 - z0;
   }
